@@ -1,0 +1,209 @@
+"""Seeded synthetic scalar fields that stand in for the SDRBench / CESM inputs.
+
+The reference publishes its timings on SDRBench fields that are not available
+offline, so every workload here is generated from a seed.  Choices that the
+workload descriptions leave open are fixed as follows:
+
+* Gaussian-bump fields: bump centres are uniform over the grid, sigma is
+  uniform in the stated range, amplitudes are N(0, 1).  Each bump is evaluated
+  separably (a rank-1 tensor per bump), summed in float64, and the low-frequency
+  term ``0.3*sin(2*pi*x/W)*cos(2*pi*y/H)`` (times ``cos(2*pi*z/D)`` in 3D) plus
+  N(0, noise) white noise is added before the cast to float32.
+* Band-limited field: white noise -> real FFT -> amplitude scaled by
+  ``k**-1.5`` (power spectrum k^-3), DC set to 0 -> inverse FFT -> min-max
+  normalised to [0, 1] -> float32.
+
+Arrays are row-major (C order); axis 0 is the slowest.  Generated fields are
+cached as raw ``.f32`` files under ``$TOPOSZP_CACHE`` (default
+``/tmp/toposzp_fields``) so that repeated runs on one machine read identical
+bytes.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+CACHE_DIR = os.environ.get("TOPOSZP_CACHE", "/tmp/toposzp_fields")
+
+
+def _cache_path(tag: str) -> str:
+    return os.path.join(CACHE_DIR, tag + ".f32")
+
+
+def _cached(tag: str, shape, make):
+    path = _cache_path(tag)
+    n = int(np.prod(shape))
+    if os.path.exists(path) and os.path.getsize(path) == 4 * n:
+        return np.fromfile(path, dtype=np.float32).reshape(shape)
+    arr = np.ascontiguousarray(make(), dtype=np.float32).reshape(shape)
+    try:
+        os.makedirs(CACHE_DIR, exist_ok=True)
+        tmp = path + ".%d.tmp" % os.getpid()
+        arr.tofile(tmp)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+    return arr
+
+
+def gaussian_bumps(shape, n_bumps, sigma_lo, sigma_hi, noise, seed,
+                   lowfreq=0.3) -> np.ndarray:
+    """Sum of separable Gaussian bumps + low-frequency trig term + noise."""
+    rng = np.random.default_rng(seed)
+    shape = tuple(int(s) for s in shape)
+    nd = len(shape)
+    centers = np.stack([rng.uniform(0, s, size=n_bumps) for s in shape], 1)
+    sigmas = rng.uniform(sigma_lo, sigma_hi, size=n_bumps)
+    amps = rng.standard_normal(n_bumps)
+    axes = [np.arange(s, dtype=np.float64) for s in shape]
+    # per-axis factor matrices G[a] of shape (s_a, n_bumps)
+    G = [np.exp(-((ax[:, None] - centers[None, :, a]) ** 2) /
+                (2.0 * sigmas[None, :] ** 2)) for a, ax in enumerate(axes)]
+    if nd == 2:
+        out = (G[0] * amps[None, :]) @ G[1].T
+    else:
+        out = np.empty(shape, dtype=np.float64)
+        A = G[0] * amps[None, :]
+        for x in range(shape[0]):
+            out[x] = (G[1] * A[x][None, :]) @ G[2].T
+    # low-frequency term: 0.3 sin(2 pi x / W) cos(2 pi y / H) [cos(2 pi z / D)]
+    trig = [np.sin(2 * np.pi * axes[-1] / shape[-1]),
+            np.cos(2 * np.pi * axes[-2] / shape[-2])]
+    if nd == 2:
+        out += lowfreq * trig[1][:, None] * trig[0][None, :]
+    else:
+        cz = np.cos(2 * np.pi * axes[0] / shape[0])
+        out += lowfreq * (cz[:, None, None] * trig[1][None, :, None] *
+                          trig[0][None, None, :])
+    if noise > 0:
+        out += rng.normal(0.0, noise, size=shape)
+    return out.astype(np.float32)
+
+
+def band_limited(shape, seed, slope=-1.5) -> np.ndarray:
+    """FFT-filtered white noise with power spectrum k^(2*slope), in [0, 1]."""
+    import scipy.fft as sfft
+    rng = np.random.default_rng(seed)
+    shape = tuple(int(s) for s in shape)
+    white = rng.standard_normal(shape)
+    spec = sfft.rfftn(white, workers=-1)
+    del white
+    freqs = [np.fft.fftfreq(s) * s for s in shape[:-1]]
+    freqs.append(np.fft.rfftfreq(shape[-1]) * shape[-1])
+    k2 = np.zeros(spec.shape, dtype=np.float64)
+    for a, f in enumerate(freqs):
+        sl = [None] * len(shape)
+        sl[a] = slice(None)
+        k2 = k2 + (f[tuple(sl)] ** 2)
+    k2.flat[0] = 1.0
+    amp = k2 ** (slope / 2.0)
+    amp.flat[0] = 0.0
+    spec *= amp
+    del k2, amp
+    out = sfft.irfftn(spec, s=shape, workers=-1)
+    del spec
+    lo, hi = out.min(), out.max()
+    out = (out - lo) / (hi - lo)
+    return out.astype(np.float32)
+
+
+@dataclass
+class Field:
+    name: str
+    dims: tuple            # (rows, cols) or (d1, d2, d3)
+    data: np.ndarray       # float32, C order, shape == dims
+    eb_mode: str           # "abs" or "rel"
+    eb_value: float        # as given (relative fraction for "rel")
+    block_size: int = 64
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return int(self.data.size)
+
+    def abs_eb(self) -> float:
+        """Absolute error bound, computed like the reference's eb parser:
+        relative bounds are ``rel * (max - min)`` in float32 arithmetic,
+        with a zero range replaced by FLT_EPSILON."""
+        if self.eb_mode == "abs":
+            return float(np.float32(self.eb_value))
+        mn = np.float32(self.data.min())
+        mx = np.float32(self.data.max())
+        rng_ = np.float32(mx - mn)
+        if not rng_ > 0:
+            rng_ = np.float32(np.finfo(np.float32).eps)
+        return float(np.float32(np.float32(self.eb_value) * rng_))
+
+    def digest(self) -> str:
+        return hashlib.sha256(self.data.tobytes()).hexdigest()[:16]
+
+
+def config1() -> Field:
+    """2D 1800x3600, 40 bumps (sigma 20-200), +0.3 sin*cos, +N(0,1e-3), seed 0."""
+    dims = (1800, 3600)
+    data = _cached("c1_1800x3600_s0", dims,
+                   lambda: gaussian_bumps(dims, 40, 20, 200, 1e-3, 0))
+    return Field("c1_2d_1800x3600", dims, data, "abs", 1e-3)
+
+
+def config2() -> Field:
+    """3D 100x500x500, 200 bumps (sigma 5-60), +N(0,1e-4), seed 1, rel 1e-4."""
+    dims = (100, 500, 500)
+    data = _cached("c2_100x500x500_s1", dims,
+                   lambda: gaussian_bumps(dims, 200, 5, 60, 1e-4, 1))
+    return Field("c2_3d_100x500x500", dims, data, "rel", 1e-4)
+
+
+def config3(side: int = 512) -> Field:
+    """3D side^3 band-limited field (power k^-3) in [0,1], seed 2, abs 1e-4."""
+    dims = (side, side, side)
+    data = _cached("c3_%d_s2" % side, dims, lambda: band_limited(dims, 2))
+    return Field("c3_3d_%d^3" % side, dims, data, "abs", 1e-4)
+
+
+def batch_specs(count: int = 256, seed: int = 3):
+    """Shapes and error bounds of the mixed-size batch (no data)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        if i < count // 2:
+            dims = tuple(int(round(math.exp(rng.uniform(math.log(64), math.log(2048)))))
+                         for _ in range(2))
+        else:
+            dims = tuple(int(round(math.exp(rng.uniform(math.log(32), math.log(256)))))
+                         for _ in range(3))
+        eb = float(math.exp(rng.uniform(math.log(1e-5), math.log(1e-2))))
+        mode = "abs" if (i % 2 == 0) else "rel"
+        specs.append((dims, mode, eb, int(rng.integers(0, 2**31 - 1))))
+    return specs
+
+
+def batch_field(spec, index: int) -> Field:
+    dims, mode, eb, fseed = spec
+    nd = len(dims)
+    nb = 20 if nd == 2 else 40
+    lo, hi = (0.02, 0.2) if nd == 2 else (0.05, 0.3)
+    side = min(dims)
+    data = gaussian_bumps(dims, nb, max(1.0, lo * side), max(2.0, hi * side),
+                          1e-3, fseed)
+    return Field("batch_%03d" % index, dims, data, mode, eb)
+
+
+def small_field(dims, seed=0, kind="bumps", noise=1e-3) -> np.ndarray:
+    """Small fields for parity tests (fast to generate)."""
+    dims = tuple(int(d) for d in dims)
+    if kind == "bumps":
+        side = min(dims)
+        return gaussian_bumps(dims, 6, max(1.0, 0.05 * side), max(2.0, 0.4 * side),
+                              noise, seed)
+    if kind == "noise":
+        rng = np.random.default_rng(seed)
+        return rng.standard_normal(dims).astype(np.float32)
+    if kind == "band":
+        return band_limited(dims, seed)
+    raise ValueError(kind)
