@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark of the TopoSZp topology path on B200.
+
+One step = one pass of the hot path over one field: fused compression
+(classification + sort positions + topology stream + sort-position stream)
+followed by fused decompression with post-processing (extremum stencils,
+enforcement, RBF saddle restoration).  Workload: the 512^3 band-limited fp32
+field (power spectrum k^-3, [0,1], seed 2), absolute error bound 1e-4,
+blockSize 64 -- the single-field bandwidth/roofline case.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1: one process per GPU under torch.distributed.run, each rank processes
+its own replica of the field (weak scaling, no data-path collective); the
+timed region is bracketed by barriers and the reported time is the max over
+ranks.  Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "toposzp-cuda_b200")
+for _p in (PKG, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+import synth  # noqa: E402
+
+METRIC = "topo-compress+decompress GB/s of fp32 input (fused round trip)"
+UNIT = "GB/s"
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU reference leg: the reference's OpenMP library + driver post-processing
+# ---------------------------------------------------------------------------
+
+def cpu_reference_run(field: np.ndarray, eb: float, B: int, threads: int):
+    """One round trip of the reference's own CPU implementation on `field`
+    (3D): find -> sort -> sort-position stream -> topology stream ->
+    decompress -> sort-position decode -> stencils -> enforcement -> RBF."""
+    import oracle as O
+    O.set_ref_threads(threads)
+    d = np.ascontiguousarray(field, dtype=np.float32)
+    t0 = time.perf_counter()
+    cp = O.ref_sort_cp(O.ref_find_cp(d, eb), d)
+    sp_stream = O.ref_compress_sp(cp, B)
+    topo = O.ref_compress_topo(d, eb, B, cp)
+    raw, fn = O.ref_decompress_topo(topo, d.size, eb, B)
+    e = int(np.count_nonzero((cp["type"] == 1) | (cp["type"] == 2)))
+    sp = O.ref_decompress_sp(sp_stream[8:], e, B) if e else None
+    out, _ = O.ref_post(raw.reshape(d.shape), raw.reshape(d.shape), fn.reshape(d.shape), sp, eb)
+    return time.perf_counter() - t0, len(topo), len(sp_stream)
+
+
+def cpu_port_run(field: np.ndarray, eb: float, B: int):
+    import oracle as O
+    d = np.ascontiguousarray(field, dtype=np.float32)
+    t0 = time.perf_counter()
+    cp = O.sort_cp(O.find_cp(d, eb), d)
+    topo = O.encode_topo(d, eb, B, O.mark_types(cp, d.shape))
+    sp = O.extract_sp(cp)
+    srt = O.encode_ints(sp, B) if len(sp) else b""
+    raw, fn, _ = O.decode_topo(topo, d.size, eb, B)
+    O.post(raw.reshape(d.shape), raw.reshape(d.shape), fn.reshape(d.shape), sp, eb)
+    return time.perf_counter() - t0, len(topo), len(srt)
+
+
+def reference_leg(f, planes, threads):
+    import oracle as O
+    sample = np.ascontiguousarray(f.data[:planes])
+    eb = f.abs_eb()
+    kind = "reference" if O.ref_available() else "port"
+    if kind == "reference":
+        t, _, _ = cpu_reference_run(sample, eb, f.block_size, threads)
+    else:
+        t, _, _ = cpu_port_run(sample, eb, f.block_size)
+        threads = 1
+    gbs = 4.0 * sample.size / t / 1e9
+    return {"value": gbs, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": "first %d of %d planes of the %s field (%d elements), full round trip "
+                      "incl. post-processing, %.2f s" % (planes, f.dims[0], f.name, sample.size, t)}
+
+
+# ---------------------------------------------------------------------------
+# main
+# ---------------------------------------------------------------------------
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--side", type=int, default=512, help="edge of the cubic field")
+    ap.add_argument("--cpu-planes", type=int, default=256, help="planes in the CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def run_reference_arm(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    f = synth.config3(args.side)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        reference_leg(f, max(4, args.cpu_planes // 4), threads)
+    vals, info = [], None
+    for _ in range(args.steps):
+        info = reference_leg(f, args.cpu_planes, threads)
+        vals.append(info["value"])
+    v = statistics.median(vals)
+    info = dict(info, value=v)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 4.0 * args.cpu_planes * args.side * args.side / v / 1e6,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded band-limited field)",
+        "config": {"workload": "%s: %d^3 band-limited fp32 field, abs eb 1e-4, blockSize 64, "
+                               "round trip with post-processing; CPU sample = first %d planes"
+                               % (f.name, args.side, args.cpu_planes),
+                   "threads": threads},
+        "cpu_baseline": info,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    import toposzp_b200 as T
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    f = synth.config3(args.side)
+    eb = f.abs_eb()
+    B = f.block_size
+    dims = f.dims
+    n = f.n
+    d_field = torch.from_numpy(f.data.reshape(-1)).to(dev)
+
+    ctx = T.Context(torch.cuda.current_stream(dev).cuda_stream)
+    L = T.lib()
+    topo = torch.empty(L.szp_b200_topo_bound(n, B), dtype=torch.uint8, device=dev)
+    sort = torch.empty(L.szp_b200_sort_bound(n, B), dtype=torch.uint8, device=dev)
+    idx = torch.empty(2 * ((n + B - 1) // B), dtype=torch.int64, device=dev)
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    import ctypes as C
+    sizes = T.Sizes()
+
+    def step():
+        rc = L.szp_b200_topo_compress_dev(ctx.ptr, C.c_void_p(d_field.data_ptr()), T.geom_of(dims), eb, B,
+                                          C.c_void_p(topo.data_ptr()), C.c_void_p(sort.data_ptr()),
+                                          C.c_void_p(idx.data_ptr()), C.byref(sizes))
+        if rc:
+            raise T.ToposzpError(T.last_error())
+        st_c = ctx.stage_times()
+        rc = L.szp_b200_topo_decompress_dev(ctx.ptr, C.c_void_p(topo.data_ptr()), sizes.topo_bytes,
+                                            C.c_void_p(sort.data_ptr()), sizes.sort_bytes,
+                                            C.c_void_p(idx.data_ptr()), T.geom_of(dims), eb, B,
+                                            C.c_void_p(out.data_ptr()), None, 1)
+        if rc:
+            raise T.ToposzpError(T.last_error())
+        return st_c + ctx.stage_times()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    stage_acc = {}
+    l0 = ctx.launches()
+    barrier(world)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            for name, ms in step():
+                stage_acc.setdefault(name, []).append(ms)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ms_local = ev0.elapsed_time(ev1) / args.steps
+    launches = ctx.launches() - l0
+    ms_step = max_over_ranks(ms_local, world)
+    value = world * 4.0 * n / (ms_step * 1e-3) / 1e9
+
+    # check the last output against the error bound (cheap, after timing)
+    err = (out - d_field).abs().max().item()
+
+    stages = {k: statistics.mean(v) for k, v in stage_acc.items()}
+    peak, peak_kind = peaks()
+    s_topo, s_sort = sizes.topo_bytes, sizes.sort_bytes
+    alg = {"encode_topo": 4.0 * n + s_topo, "decode_topo": s_topo + 4.0 * n,
+           "encode_sort": 4.0 * sizes.extrema_count + s_sort,
+           "decode_sort": s_sort + 4.0 * sizes.extrema_count}
+    dom = max(stages, key=stages.get)
+    # roofline of the dominant codec kernel (the stage with algorithmic bytes
+    # and the largest share); the dominant stage overall is reported beside it
+    codec = max([k for k in alg if k in stages], key=lambda k: stages[k])
+    achieved = alg[codec] / (stages[codec] * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            with open(prof) as fh:
+                traffic = json.load(fh).get(codec)
+        except Exception:
+            traffic = None
+    rt_bytes = 2.0 * (4.0 * n + s_topo + s_sort)
+    roofline = {"bound": "hbm", "kernel": codec, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg[codec], "ms_per_launch": stages[codec],
+                "round_trip": {"algorithmic_bytes": rt_bytes,
+                               "achieved": rt_bytes / (ms_step * 1e-3) / 1e9,
+                               "frac": rt_bytes / (ms_step * 1e-3) / 1e9 / peak},
+                "dominant_stage": dom}
+
+    # end to end through the host-buffer C ABI: pinned field in, streams out,
+    # streams in, post-processed field out
+    e2e = None
+    if not args.no_e2e:
+        h_field = torch.from_numpy(f.data.reshape(dims)).pin_memory()
+        h_topo = torch.empty(L.szp_b200_topo_bound(n, B), dtype=torch.uint8).pin_memory()
+        h_sort = torch.empty(L.szp_b200_sort_bound(n, B), dtype=torch.uint8).pin_memory()
+        h_out = torch.empty(dims, dtype=torch.float32).pin_memory()
+        hf, ht, hs, ho = (h_field.numpy(), h_topo.numpy(), h_sort.numpy(), h_out.numpy())
+        ectx = T.Context(torch.cuda.current_stream(dev).cuda_stream)
+
+        def e2e_step():
+            sz = ectx.compress_host(hf, eb, B, ht, hs)
+            ectx.decompress_host(ht, sz.topo_bytes, hs, sz.sort_bytes, dims, eb, B, ho, 1)
+            return sz
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ke = max(2, min(args.steps, 3))
+        for _ in range(ke):
+            sz = e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e_ms = max_over_ranks(e0.elapsed_time(e1) / ke, world)
+        same = bool(np.array_equal(ho.reshape(-1).view(np.int32), out.cpu().numpy().view(np.int32)))
+        e2e = {"value": world * 4.0 * n / (e_ms * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * n + sz.topo_bytes + sz.sort_bytes,
+               "d2h_bytes_per_step": sz.topo_bytes + sz.sort_bytes + 4 * n,
+               "ms_per_step": e_ms, "matches_device_path": same,
+               "wall_ms_per_step": (time.perf_counter() - t0) * 1e3 / ke}
+        ectx.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = reference_leg(f, args.cpu_planes, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded band-limited field, FFT-filtered noise k^-3, seed 2)",
+            "config": {"workload": "%s: %dx%dx%d fp32, abs eb %g, blockSize %d, fused compress + "
+                                   "decompress + post-processing per step"
+                                   % (f.name, dims[0], dims[1], dims[2], eb, B),
+                       "l2": "input (%.0f MB) larger than L2 (126 MB)" % (4 * n / 1e6),
+                       "parallelism": "replicas (one field per GPU)" if world > 1 else "single GPU",
+                       "cps": sizes.cp_count, "extrema": sizes.extrema_count,
+                       "topo_bytes": s_topo, "sort_bytes": s_sort,
+                       "compression_ratio": 4.0 * n / (s_topo + s_sort),
+                       "max_abs_err_over_eb": err / eb},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "stages_ms": stages,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,205 @@
+/*
+ * szp_b200.h -- C ABI of the B200-native TopoSZp topology path.
+ *
+ * Part 1 re-exports the reference's topology entry points with identical
+ * names, argument lists, struct layouts and byte-stream layout, so a caller
+ * linked against the reference CUDA library can relink against
+ * libtoposzp_b200.so unchanged.  Host pointers in, malloc'd host buffers out
+ * (release them with free()), exactly as in the reference.
+ *
+ * Deviation: where the reference calls exit(EXIT_FAILURE) (bad blockSize or
+ * dimensions, any CUDA error), these functions return NULL / a zero count and
+ * record a message that szp_b200_last_error() returns.
+ *
+ * Part 2 adds device-pointer entry points (fused compress / decompress /
+ * post-processing on a caller stream) that have no counterpart in the
+ * reference.
+ */
+#ifndef SZP_B200_H
+#define SZP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SZP_B200_API __attribute__((visibility("default")))
+#else
+#define SZP_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* ABI structs (SZp/include/szp_float.h:20-25, SZp/include/szp_topology_3d.h:22-27) */
+/* ------------------------------------------------------------------ */
+#ifndef _szp_Float_H
+typedef struct {
+    int x, y;
+    int type;            /* 1 max, 2 min, 3 saddle */
+    int quantized_bin;
+    int sort_position;
+} CriticalPoint;
+#endif
+
+#ifndef _SZP_TOPOLOGY_3D_H
+typedef struct {
+    int x, y, z;
+    int type;
+    int quantized_bin;
+    int sort_position;
+} CriticalPoint3D;
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Part 1: reference entry points                                      */
+/* ------------------------------------------------------------------ */
+
+/* replaces SZp/include/szp_cuda_topology.cuh:23-24 (szp_cuda_topology.cu:78) */
+SZP_B200_API CriticalPoint *szp_cuda_find_critical_points(float *data, size_t *outCount,
+                                              int rows, int cols, float absErrBound);
+
+/* replaces SZp/include/szp_cuda_topology.cuh:30-32 (szp_cuda_topology.cu:195) */
+SZP_B200_API void szp_cuda_sort_critical_points_by_original_data(CriticalPoint *critical_points,
+                                                     size_t critical_count,
+                                                     float *data, int cols);
+
+/* replaces SZp/include/szp_cuda_topology.cuh:38-40 (szp_cuda_topology.cu:424) */
+SZP_B200_API unsigned char *szp_cuda_compress_sort_positions(CriticalPoint *critical_points,
+                                                 size_t critical_count,
+                                                 size_t *outSize, int blockSize);
+
+/* replaces SZp/include/szp_cuda_topology.cuh:46-50 (szp_cuda_topology.cu:683) */
+SZP_B200_API unsigned char *szp_cuda_float_compress_randomaccess_topology_preserved(
+    float *oriData, size_t *outSize, float absErrBound,
+    size_t nbEle, int blockSize,
+    CriticalPoint *critical_points, int critical_count,
+    int rows, int cols);
+
+/* replaces SZp/include/szp_cuda_topology_3d.cuh:16-18 (szp_cuda_topology_3d.cu:175) */
+SZP_B200_API CriticalPoint3D *szp_cuda_find_critical_points_3d(float *data, size_t *outCount,
+                                                    int d1, int d2, int d3,
+                                                    float absErrBound);
+
+/* replaces SZp/include/szp_cuda_topology_3d.cuh:20-22 (szp_cuda_topology_3d.cu:321) */
+SZP_B200_API void szp_cuda_sort_critical_points_3d(CriticalPoint3D *critical_points,
+                                       size_t critical_count,
+                                       float *data, int d2, int d3);
+
+/* replaces SZp/include/szp_cuda_topology_3d.cuh:24-26 (szp_cuda_topology_3d.cu:529) */
+SZP_B200_API unsigned char *szp_cuda_compress_sort_positions_3d(CriticalPoint3D *critical_points,
+                                                     size_t critical_count,
+                                                     size_t *outSize, int blockSize);
+
+/* replaces SZp/include/szp_cuda_topology_3d.cuh:28-32 (szp_cuda_topology_3d.cu:958) */
+SZP_B200_API unsigned char *szp_cuda_float_compress_topology_3d(
+    float *oriData, size_t *outSize, float absErrBound,
+    size_t nbEle, int blockSize,
+    CriticalPoint3D *critical_points, int critical_count,
+    int d1, int d2, int d3);
+
+/* replaces SZp/include/szp_cuda_decompress.cuh:63-65 (szp_cuda_decompress.cu:1074) */
+SZP_B200_API void szp_cuda_float_decompress_randomaccess_topology_preserved(
+    float **newData, size_t nbEle, float absErrBound, int blockSize,
+    unsigned char *cmpBytes, int **FN);
+
+/* replaces SZp/include/szp_cuda_decompress.cuh:71-72 (szp_cuda_decompress.cu:1165) */
+SZP_B200_API int *szp_cuda_decompress_sort_positions(
+    unsigned char *cmpBytes, size_t critical_count, int blockSize);
+
+/* ------------------------------------------------------------------ */
+/* Part 2: additions (no reference counterpart)                        */
+/* ------------------------------------------------------------------ */
+
+/* Message of the last failure on this thread ("" when none). */
+SZP_B200_API const char *szp_b200_last_error(void);
+
+/* Library version string. */
+SZP_B200_API const char *szp_b200_version(void);
+
+/* Opaque, reusable device workspace (scratch buffers, stream, events). */
+typedef struct szp_b200_ctx szp_b200_ctx;
+
+/* Create / destroy a workspace on the current device.  stream may be 0. */
+SZP_B200_API szp_b200_ctx *szp_b200_ctx_create(void *cuda_stream);
+SZP_B200_API void szp_b200_ctx_destroy(szp_b200_ctx *ctx);
+
+/* Device time of each stage of the last call on this workspace, measured
+ * with CUDA events on the workspace stream.  Fills up to max entries and
+ * returns how many stages the call had. */
+SZP_B200_API int szp_b200_ctx_stage_times(szp_b200_ctx *ctx, const char **names, float *ms, int max);
+
+/* Number of kernels this workspace has launched since it was created. */
+SZP_B200_API unsigned long long szp_b200_ctx_launches(szp_b200_ctx *ctx);
+
+/* Geometry of a field: nd = 2 (dims[0] rows, dims[1] cols) or nd = 3. */
+typedef struct {
+    int nd;
+    int dims[3];
+} szp_b200_geom;
+
+/* Result of a fused compression, all sizes in bytes. */
+typedef struct {
+    size_t topo_bytes;      /* topology stream, header included */
+    size_t sort_bytes;      /* sort-position stream, header included (0 if no extrema) */
+    size_t cp_count;        /* critical points */
+    size_t extrema_count;   /* maxima + minima */
+} szp_b200_sizes;
+
+/* Upper bounds of the two streams for n elements (for sizing buffers). */
+SZP_B200_API size_t szp_b200_topo_bound(size_t n, int blockSize);
+SZP_B200_API size_t szp_b200_sort_bound(size_t n, int blockSize);
+
+/* Fused compression of a device-resident field: classify, rank, pack.
+ *   d_data        device float[n]
+ *   d_topo        device buffer >= szp_b200_topo_bound(n, B)
+ *   d_sort        device buffer >= szp_b200_sort_bound(n, B)
+ *   d_blk_index   optional device uint64[2 * ceil(n/B)]: payload offset of
+ *                 every topology block, followed by the offsets of the
+ *                 sort-position blocks; szp_b200_topo_decompress_dev reuses it
+ * Synchronous on the workspace stream.  Returns 0 on success. */
+SZP_B200_API int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_data,
+                               szp_b200_geom geom, float absErrBound, int blockSize,
+                               unsigned char *d_topo, unsigned char *d_sort,
+                               uint64_t *d_blk_index, szp_b200_sizes *sizes);
+
+/* Fused decompression + post-processing of device-resident streams.
+ *   d_blk_index   block index written by szp_b200_topo_compress_dev (required)
+ *   d_out         device float[n] (output)
+ *   d_types       optional device uint8[n] (2-bit tags, output)
+ *   postprocess   0: raw decode only; 1: stencils + enforcement + RBF;
+ *                 2: as 1 plus the 3D axis-pattern saddle stencil */
+SZP_B200_API int szp_b200_topo_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_topo,
+                                 size_t topo_bytes, const unsigned char *d_sort,
+                                 size_t sort_bytes, const uint64_t *d_blk_index,
+                                 szp_b200_geom geom, float absErrBound, int blockSize,
+                                 float *d_out, unsigned char *d_types, int postprocess);
+
+/* Host-buffer forms of the two calls above: the field and the streams live
+ * in host memory (pinned memory gives full copy bandwidth); device staging
+ * is kept in the workspace.  The decompressor finds the block offsets from
+ * the stream bytes alone, as the reference decoder does. */
+SZP_B200_API int szp_b200_topo_compress_host(szp_b200_ctx *ctx, const float *h_data,
+                                szp_b200_geom geom, float absErrBound, int blockSize,
+                                unsigned char *h_topo, size_t topo_cap,
+                                unsigned char *h_sort, size_t sort_cap,
+                                szp_b200_sizes *sizes);
+SZP_B200_API int szp_b200_topo_decompress_host(szp_b200_ctx *ctx, const unsigned char *h_topo,
+                                  size_t topo_bytes, const unsigned char *h_sort,
+                                  size_t sort_bytes, szp_b200_geom geom, float absErrBound,
+                                  int blockSize, float *h_out, int postprocess);
+
+/* Post-processing of an already decoded field in place (device pointers).
+ *   d_orig   raw decoded values (read only)
+ *   d_types  int per element (FN) as returned by the reference decoder
+ *   d_sp     decoded sort positions (E entries), may be NULL when E == 0 */
+SZP_B200_API int szp_b200_topo_postprocess_dev(szp_b200_ctx *ctx, float *d_data, const float *d_orig,
+                                  const int *d_types, const int *d_sp, size_t n_sp,
+                                  szp_b200_geom geom, float absErrBound, int axis_stencil);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SZP_B200_H */

@@ -1,0 +1,189 @@
+"""GPU parity of the C ABI against the oracle (bit-exact).
+
+Every check goes through libtoposzp_b200.so: the reference-compatible entry
+points (host buffers) and the fused device entry points (torch CUDA tensors).
+Integer / byte outputs and decoded / post-processed floats must be identical
+to the oracle's, bit for bit.
+"""
+import numpy as np
+import pytest
+
+import synth
+
+pytestmark = pytest.mark.gpu
+
+CASES_2D = [
+    # dims, eb, B, kind, scale
+    ((37, 53), 1e-3, 64, "bumps", 1.0),
+    ((64, 80), 1e-2, 64, "noise", 0.1),
+    ((60, 90), 1e-2, 16, "bumps", 1.0),
+    ((33, 31), 1e-3, 7, "bumps", 1.0),
+    ((5, 13), 1e-3, 64, "noise", 1.0),        # n % B == 1: anchor-only tail block
+    ((40, 45), 0.05, 1, "noise", 0.1),        # blockSize 1
+    ((41, 47), 1e-3, 257, "noise", 1.0),      # largest blockSize
+    ((3, 3), 1e-3, 64, "noise", 1.0),
+    ((50, 70), 1e-5, 64, "noise", 1e3),       # wide deltas: bit counts > 24
+    ((30, 30), 1e-9, 32, "noise", 1e3),       # quantization saturates the int range
+    ((180, 360), 1e-3, 64, "bumps", 1.0),
+]
+
+CASES_3D = [
+    ((12, 20, 17), 1e-3, 64, "bumps", 1.0),
+    ((16, 18, 20), 0.02, 64, "noise", 1.0),
+    ((20, 24, 28), 1e-3, 64, "band", 1.0),
+    ((9, 9, 9), 1e-4, 8, "bumps", 1.0),
+    ((3, 3, 3), 1e-3, 64, "noise", 1.0),
+    ((7, 5, 13), 1e-2, 64, "noise", 0.1),     # 455 % 64 == 7
+    ((40, 50, 60), 1e-3, 64, "bumps", 1.0),   # the reference's own 3D test shape
+]
+
+
+def field(dims, kind, scale, seed=7):
+    d = synth.small_field(dims, seed=seed, kind=kind)
+    return (d * np.float32(scale)).astype(np.float32)
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.int32)
+
+
+@pytest.fixture(scope="module")
+def T(ora):
+    import torch
+    import toposzp_b200
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    toposzp_b200.lib()
+    return toposzp_b200
+
+
+@pytest.mark.parametrize("case", CASES_2D + CASES_3D, ids=lambda c: "x".join(map(str, c[0])) + "_B%d" % c[2])
+def test_reference_api_parity(T, ora, case):
+    dims, eb, B, kind, scale = case
+    d = field(dims, kind, scale)
+    # find
+    cp = T.find_critical_points(d, eb)
+    ocp = ora.find_cp(d, eb)
+    assert len(cp) == len(ocp)
+    assert (cp == ocp).all()
+    if len(ocp) == 0:
+        return
+    # sort positions (of the oracle's list: the entry point ranks any list)
+    scp = T.sort_critical_points(ocp, d)
+    oscp = ora.sort_cp(ocp, d)
+    assert (scp == oscp).all()
+    # topology stream
+    types = ora.mark_types(oscp, dims)
+    s_gpu = T.compress_topology(d, eb, B, oscp)
+    s_ora = ora.encode_topo(d, eb, B, types)
+    assert s_gpu == s_ora
+    # sort-position stream
+    sp = ora.extract_sp(oscp)
+    sp_gpu = T.compress_sort_positions(oscp, B)
+    sp_ora = ora.encode_ints(sp, B) if len(sp) else b""
+    assert sp_gpu == sp_ora
+    # decode
+    out, fn = T.decompress_topology(s_gpu, d.size, eb, B)
+    oout, ofn, used = ora.decode_topo(s_ora, d.size, eb, B)
+    assert used == len(s_ora)
+    assert (bits(out) == bits(oout)).all()
+    assert (fn == ofn).all()
+    if len(sp):
+        dsp = T.decompress_sort_positions(sp_gpu, len(sp), B)
+        assert (dsp == sp).all()
+    # raw error bound (reference tests use 1.01 eb) where float32 can resolve eb
+    if np.abs(d).max() * (1.0 / eb) < 2e9 and np.spacing(np.float32(np.abs(d).max())) < 0.01 * eb:
+        assert np.abs(out.astype(np.float64) - d.reshape(-1)).max() <= 1.01 * eb
+
+
+@pytest.mark.parametrize("case", CASES_2D + CASES_3D, ids=lambda c: "x".join(map(str, c[0])) + "_B%d" % c[2])
+def test_fused_device_parity(T, ora, case):
+    import torch
+    dims, eb, B, kind, scale = case
+    d = field(dims, kind, scale)
+    ctx = T.Context()
+    dd = torch.from_numpy(d.reshape(-1).copy()).cuda()
+    topo, sort, idx, sizes = ctx.compress(dd, dims, eb, B)
+    ocp = ora.sort_cp(ora.find_cp(d, eb), d)
+    types = ora.mark_types(ocp, dims)
+    s_ora = ora.encode_topo(d, eb, B, types)
+    sp = ora.extract_sp(ocp)
+    assert sizes.cp_count == len(ocp)
+    assert sizes.extrema_count == len(sp)
+    assert sizes.topo_bytes == len(s_ora)
+    assert topo[: sizes.topo_bytes].cpu().numpy().tobytes() == s_ora
+    if len(sp):
+        assert sort[: sizes.sort_bytes].cpu().numpy().tobytes() == ora.encode_ints(sp, B)
+    else:
+        assert sizes.sort_bytes == 0
+    # raw decode
+    raw = ctx.decompress(topo, sizes.topo_bytes, sort, sizes.sort_bytes, idx, dims, eb, B,
+                         postprocess=0)
+    oraw, ofn, _ = ora.decode_topo(s_ora, d.size, eb, B)
+    assert (bits(raw.cpu().numpy()) == bits(oraw)).all()
+    # decode + post-processing
+    for mode in ([1, 2] if len(dims) == 3 else [1]):
+        tys = torch.empty(d.size, dtype=torch.uint8, device="cuda")
+        post = ctx.decompress(topo, sizes.topo_bytes, sort, sizes.sort_bytes, idx, dims, eb, B,
+                              postprocess=mode, types=tys)
+        ref, _ = ora.post(oraw.reshape(dims), oraw.reshape(dims), ofn.reshape(dims), sp, eb,
+                          axis_stencil=(mode == 2))
+        got = post.cpu().numpy()
+        mism = np.nonzero(bits(got) != bits(ref.reshape(-1)))[0]
+        assert mism.size == 0, "post mode %d: %d mismatches, first %s" % (mode, mism.size, mism[:5])
+        assert (tys.cpu().numpy() == ofn.astype(np.uint8)).all()
+    ctx.close()
+
+
+@pytest.mark.parametrize("case", [c for c in CASES_2D + CASES_3D if np.prod(c[0]) >= 27],
+                         ids=lambda c: "x".join(map(str, c[0])))
+def test_postprocess_entry_parity(T, ora, case):
+    """szp_b200_topo_postprocess_dev on the reference decoder's outputs."""
+    import torch
+    dims, eb, B, kind, scale = case
+    d = field(dims, kind, scale, seed=11)
+    ocp = ora.sort_cp(ora.find_cp(d, eb), d)
+    types = ora.mark_types(ocp, dims)
+    raw, fn, _ = ora.decode_topo(ora.encode_topo(d, eb, B, types), d.size, eb, B)
+    sp = ora.extract_sp(ocp)
+    ctx = T.Context()
+    for axis in ([False, True] if len(dims) == 3 else [False]):
+        f = torch.from_numpy(raw.copy()).cuda()
+        o = torch.from_numpy(raw.copy()).cuda()
+        t = torch.from_numpy(fn.copy()).cuda()
+        s = torch.from_numpy(sp.copy()).cuda() if len(sp) else None
+        ctx.postprocess(f, o, t, s, dims, eb, axis_stencil=axis)
+        ref, _ = ora.post(raw.reshape(dims), raw.reshape(dims), fn.reshape(dims), sp, eb,
+                          axis_stencil=axis)
+        assert (bits(f.cpu().numpy()) == bits(ref.reshape(-1))).all()
+    ctx.close()
+
+
+def test_bitcount_matches_host_log2f(T, ora):
+    """The device bit count floor(log2f(m))+1 equals the host one for every
+    magnitude of a full block sweep (both through the codec)."""
+    # magnitudes around every power of two up to 2^31, packed as consecutive deltas
+    mags = []
+    for k in range(1, 32):
+        for dm in (-3, -2, -1, 0, 1, 2):
+            m = (1 << k) + dm
+            if 0 < m < 2**31:
+                mags.append(m)
+    v = np.zeros(2 * len(mags), dtype=np.int64)
+    v[1::2] = mags
+    v = v.astype(np.int32)
+    import oracle as O
+    cp = np.zeros(len(v), dtype=O.CP2_DT)
+    cp["type"] = 1
+    cp["sort_position"] = v
+    got = T.compress_sort_positions(cp, 2)
+    assert got == O.encode_ints(v, 2)
+
+
+def test_errors_do_not_exit(T):
+    """Invalid arguments return NULL with a message instead of exiting."""
+    d = np.zeros((8, 8), dtype=np.float32)
+    with pytest.raises(T.ToposzpError):
+        T.compress_topology(d, 1e-3, 300, np.zeros(0, dtype=T.CP2_DT))
+    with pytest.raises(T.ToposzpError):
+        T.compress_topology(d, -1.0, 64, np.zeros(0, dtype=T.CP2_DT))

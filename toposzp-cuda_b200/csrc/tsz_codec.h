@@ -1,0 +1,55 @@
+// Internal interface of the codec kernels (not part of the C ABI).
+#pragma once
+#include "tsz_common.cuh"
+
+namespace tsz {
+
+enum EncMode { kEncClassify = 0, kEncTypes = 1, kEncInts = 2 };
+enum CpMode { kCpNone = 0, kCpRecords = 1, kCpPairs = 2 };
+
+struct EncArgs {
+  const float *data;            // float field (kEncClassify / kEncTypes)
+  const int *ints;              // int values (kEncInts)
+  const unsigned char *types;   // per-element types 0..3 (kEncTypes)
+  unsigned long long n;
+  int B;
+  float eb;
+  double inv;
+  Geom g;                       // geometry for in-kernel classification
+  unsigned char *out;           // payload base (stream + 8-byte header)
+  unsigned long long out_cap;
+  unsigned long long *blk_off;  // per-block payload offsets (optional)
+  TileDesc *desc;               // zeroed, one per tile
+  unsigned *tile_ctr;           // zeroed
+  int *err;                     // status word
+  unsigned long long *total;    // [payload bytes, cps, extrema]
+  int cp_mode;                  // CpMode (kEncClassify only)
+  void *cp_out;                 // CriticalPoint / CriticalPoint3D records or uint2 pairs
+  unsigned long long cp_cap;
+};
+
+struct DecArgs {
+  const unsigned char *payload; // stream payload (after the offset table)
+  unsigned long long payload_len;
+  const unsigned long long *blk_off;  // per-block payload offsets
+  unsigned long long n;
+  int B;
+  float eb;
+  float *out_f;                 // decoded floats (topology stream)
+  int *out_i;                   // decoded ints (sort-position stream)
+  int *fn_i;                    // 2-bit tags as int (optional)
+  unsigned char *fn_u8;         // 2-bit tags as bytes (optional)
+  int *err;
+  unsigned long long *ext_count;  // optional: number of type-1/2 tags
+  unsigned long long img_cap;   // set by the launcher
+};
+
+int kmax_for(int B);
+int bpw_for(int kmax);
+int tile_blocks_for(int B);
+size_t enc_smem_bytes(int B, bool tags);
+size_t dec_smem_bytes(int B, bool tags);
+cudaError_t launch_encode(int mode, const EncArgs &a, cudaStream_t s, int grid);
+cudaError_t launch_decode(bool tags, DecArgs a, cudaStream_t s);
+
+}  // namespace tsz

@@ -1,0 +1,44 @@
+// Internal operators shared by the API layer (not part of the C ABI).
+#pragma once
+#include "tsz_codec.h"
+#include "tsz_runtime.h"
+
+namespace tsz {
+
+// Geometry from extents (nd = 2: rows, cols; nd = 3: d1, d2, d3).
+Geom make_geom(int nd, long long a, long long b, long long c);
+
+// Runs one encoder pass on ctx->stream and waits for it.
+//   out: payload destination (stream base + 8); the 8-byte header is written here too.
+//   totals_out (host): payload bytes, cps, extrema.
+int encode_pass(szp_b200_ctx *ctx, int mode, const float *d_data, const int *d_ints,
+                const unsigned char *d_types, unsigned long long n, int B, float eb,
+                const Geom &g, unsigned char *d_stream, unsigned long long stream_cap,
+                unsigned long long *d_blk_off, int cp_mode, void *d_cp, unsigned long long cp_cap,
+                unsigned long long totals_out[3]);
+
+// Dense rank of every extremum inside its quantization bin.
+//   pairs[k] = (orderable value code, extremum index or kNoExtremum), k < K
+//   writes sp[e] for every extremum e < E.  bins come from the value
+//   (bin = quant_bin(value, eb)); mode_given_bins = true uses bins[k] instead.
+int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
+                   unsigned long long K, unsigned long long E, float eb, int *d_sp);
+
+// Post-processing of a decoded field in place (serial raster semantics of the
+// reference drivers).  types: u8 per element (or int when types_i != null).
+int postprocess(szp_b200_ctx *ctx, float *d_data, const float *d_orig,
+                const unsigned char *d_types_u8, const int *d_types_i, const int *d_sp,
+                unsigned long long n_sp, const Geom &g, float eb, int axis_stencil,
+                int *restored_out);
+
+size_t rank_scratch_bytes(unsigned long long K, int sm_count);
+size_t post_scratch_bytes(unsigned long long n);
+int compact_extrema(szp_b200_ctx *ctx, const int *d_cps, int stride, unsigned long long K, int *d_sp,
+                    unsigned long long *E_out);
+unsigned long long *post_words(szp_b200_ctx *ctx, unsigned long long n);
+int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsigned char *d_T,
+                     unsigned long long *d_S, TileDesc *desc, const int *d_sp,
+                     unsigned long long n_sp, const Geom &g, float eb, int axis_stencil,
+                     int *restored_out);
+
+}  // namespace tsz

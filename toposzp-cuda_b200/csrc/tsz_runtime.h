@@ -1,0 +1,72 @@
+// Host runtime: per-thread error state, device workspaces and scratch arenas.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "../../include/szp_b200.h"
+
+namespace tsz {
+
+void set_error(const char *fmt, ...);
+void clear_error();
+const char *last_error();
+
+// Grow-only device scratch arena, carved per call with 256-byte alignment.
+struct Arena {
+  unsigned char *base = nullptr;
+  size_t cap = 0;
+  size_t used = 0;
+  bool reserve(size_t bytes);   // ensures capacity (may reallocate; contents lost)
+  void reset() { used = 0; }
+  template <class T> T *take(size_t count) {
+    size_t bytes = (count * sizeof(T) + 255) & ~(size_t)255;
+    if (used + bytes > cap) return nullptr;
+    T *p = reinterpret_cast<T *>(base + used);
+    used += bytes;
+    return p;
+  }
+  void release();
+};
+
+}  // namespace tsz
+
+struct szp_b200_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  tsz::Arena scratch;       // per-call temporaries
+  tsz::Arena io;            // device copies of host inputs / outputs (API path)
+  unsigned long long *h_words = nullptr;   // pinned host words for small D2H reads
+  unsigned long long *d_words = nullptr;   // device status words
+  unsigned long long *post_S = nullptr;    // post-processing result words (generation-tagged)
+  unsigned long long post_S_cap = 0;
+  unsigned post_gen = 0;
+  // stage timeline of the last call (CUDA events on the workspace stream)
+  static constexpr int kMaxStages = 24;
+  cudaEvent_t ev[kMaxStages + 1] = {};
+  const char *stage_name[kMaxStages] = {};
+  int nstage = 0;
+  bool timeline_started = false;
+  unsigned long long launches = 0;         // kernels launched through this workspace
+};
+
+namespace tsz {
+
+// Per-thread default workspace used by the reference-compatible entry points.
+szp_b200_ctx *default_ctx();
+
+// Stage timeline: tl_begin() at the start of a call, tl_mark(name) after
+// each stage's work has been enqueued on ctx->stream.
+void tl_begin(szp_b200_ctx *ctx);
+void tl_mark(szp_b200_ctx *ctx, const char *name);
+
+// Rounds a byte count up to 256.
+inline size_t a256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// CUDA error -> message; returns true on failure.
+bool cuda_fail(cudaError_t e, const char *what);
+
+}  // namespace tsz

@@ -1,0 +1,623 @@
+// Sort positions: dense rank of a critical point's value among the distinct
+// values of all critical points in the same quantization bin
+// (SZp/src/szp_float.cc:137-509; SZp/src/szp_cuda_topology.cu:139-272).
+//
+// No comparison sort of all K points.  Instead:
+//   1. bucket the points by  bin mod NB  (matrix histogram -> column scan ->
+//      scatter; the order inside a bucket is irrelevant because ties share a
+//      rank);
+//   2. rank every bucket inside one CTA: the bins of a bucket are slots, each
+//      slot gets a shared-memory bitmap over its [min code, max code] range,
+//      every point sets the bit of its value code, and the dense rank is the
+//      popcount of the bits below its own code;
+//   3. buckets whose slots do not fit (bins spanning huge code ranges, e.g.
+//      values next to zero, or too many bins) fall back to a device-wide LSD
+//      radix sort on (bin, code) followed by a segmented distinct count.
+#include <algorithm>
+#include <vector>
+
+#include "tsz_ops.h"
+#include "tsz_lookback.cuh"
+
+namespace tsz {
+
+constexpr int kRankThreads = 256;
+constexpr int kMaxSlots = 256;
+constexpr int kBitmapWords = 5120;   // 20 KB bitmap + 20 KB prefix per CTA
+
+struct RankRec {
+  uint32_t code;
+  uint32_t dest;
+  int bin;
+};
+
+__device__ __forceinline__ int rec_bin(const uint2 &p, const int *bins, unsigned long long k,
+                                       float eb, double inv) {
+  return bins ? bins[k] : quant_bin(code_float(p.x), eb, inv);
+}
+
+// ---- 1a. per-CTA bucket histogram over a contiguous chunk -----------------
+__global__ void bucket_hist_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
+                                   unsigned long long K, float eb, double inv, int logNB,
+                                   unsigned long long chunk, unsigned *__restrict__ M) {
+  extern __shared__ unsigned sh[];
+  const int NB = 1 << logNB;
+  for (int b = threadIdx.x; b < NB; b += blockDim.x) sh[b] = 0;
+  __syncthreads();
+  const unsigned long long c0 = blockIdx.x * chunk;
+  const unsigned long long c1 = (c0 + chunk < K) ? c0 + chunk : K;
+  for (unsigned long long k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
+    const int bin = rec_bin(pairs[k], bins, k, eb, inv);
+    atomicAdd(&sh[(unsigned)bin & (unsigned)(NB - 1)], 1u);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < NB; b += blockDim.x) M[(size_t)blockIdx.x * NB + b] = sh[b];
+}
+
+// ---- 1b. column scan: M[g][b] <- exclusive prefix over g; tot[b] ----------
+__global__ void bucket_colscan_kernel(unsigned *__restrict__ M, int G, int NB,
+                                      unsigned *__restrict__ tot) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= NB) return;
+  unsigned run = 0;
+  for (int g = 0; g < G; g++) {
+    const unsigned v = M[(size_t)g * NB + b];
+    M[(size_t)g * NB + b] = run;
+    run += v;
+  }
+  tot[b] = run;
+}
+
+// ---- 1c. exclusive scan of bucket totals (one CTA) -------------------------
+__global__ void bucket_start_kernel(const unsigned *__restrict__ tot, int NB,
+                                    unsigned long long *__restrict__ start) {
+  __shared__ unsigned long long part[1024];
+  const int per = (NB + blockDim.x - 1) / blockDim.x;
+  const int b0 = threadIdx.x * per;
+  unsigned long long s = 0;
+  for (int i = 0; i < per; i++) if (b0 + i < NB) s += tot[b0 + i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+    unsigned long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  unsigned long long run = part[threadIdx.x] - s;
+  for (int i = 0; i < per; i++)
+    if (b0 + i < NB) { start[b0 + i] = run; run += tot[b0 + i]; }
+  if (threadIdx.x == blockDim.x - 1) start[NB] = part[threadIdx.x];
+}
+
+// ---- 1d. scatter into buckets ----------------------------------------------
+__global__ void bucket_scatter_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
+                                      unsigned long long K, float eb, double inv, int logNB,
+                                      unsigned long long chunk, const unsigned *__restrict__ M,
+                                      const unsigned long long *__restrict__ start,
+                                      RankRec *__restrict__ recs) {
+  extern __shared__ unsigned sh[];
+  const int NB = 1 << logNB;
+  for (int b = threadIdx.x; b < NB; b += blockDim.x) sh[b] = M[(size_t)blockIdx.x * NB + b];
+  __syncthreads();
+  const unsigned long long c0 = blockIdx.x * chunk;
+  const unsigned long long c1 = (c0 + chunk < K) ? c0 + chunk : K;
+  for (unsigned long long k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
+    const uint2 p = pairs[k];
+    const int bin = rec_bin(p, bins, k, eb, inv);
+    const unsigned b = (unsigned)bin & (unsigned)(NB - 1);
+    const unsigned local = atomicAdd(&sh[b], 1u);
+    RankRec r;
+    r.code = p.x;
+    r.dest = p.y;
+    r.bin = bin;
+    recs[start[b] + local] = r;
+  }
+}
+
+// ---- 2. per-bucket bitmap rank ---------------------------------------------
+__device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v, unsigned long long *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  unsigned long long t = 0;
+  for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += red[i];
+  return t;
+}
+
+__global__ void __launch_bounds__(kRankThreads)
+bucket_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *__restrict__ start,
+                   int logNB, int *__restrict__ out, unsigned *__restrict__ fb_list,
+                   unsigned *__restrict__ fb_count) {
+  __shared__ unsigned s_min[kMaxSlots], s_max[kMaxSlots], s_wbase[kMaxSlots + 1];
+  __shared__ unsigned bm[kBitmapWords];
+  __shared__ unsigned pref[kBitmapWords];
+  __shared__ int s_bmin, s_bmax;
+  __shared__ unsigned s_total_words;
+  __shared__ int s_fail;
+  const unsigned b = blockIdx.x;
+  const unsigned long long r0 = start[b], r1 = start[b + 1];
+  if (r1 == r0) return;
+  const unsigned long long cnt = r1 - r0;
+  if (threadIdx.x == 0) { s_bmin = 0x7fffffff; s_bmax = (int)0x80000000; s_fail = 0; }
+  __syncthreads();
+  int lmin = 0x7fffffff, lmax = (int)0x80000000;
+  for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const int bin = recs[r0 + i].bin;
+    lmin = min(lmin, bin);
+    lmax = max(lmax, bin);
+  }
+  atomicMin(&s_bmin, lmin);
+  atomicMax(&s_bmax, lmax);
+  __syncthreads();
+  const long long span = ((long long)s_bmax - (long long)s_bmin) >> logNB;
+  if (span + 1 > kMaxSlots) {
+    if (threadIdx.x == 0) fb_list[atomicAdd(fb_count, 1u)] = b;
+    return;
+  }
+  const int nslots = (int)span + 1;
+  for (int s = threadIdx.x; s < nslots; s += blockDim.x) { s_min[s] = 0xffffffffu; s_max[s] = 0u; }
+  __syncthreads();
+  const int bmin = s_bmin;
+  for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const RankRec r = recs[r0 + i];
+    const int s = (int)(((long long)r.bin - bmin) >> logNB);
+    atomicMin(&s_min[s], r.code);
+    atomicMax(&s_max[s], r.code);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long w = 0;
+    for (int s = 0; s < nslots; s++) {
+      s_wbase[s] = (unsigned)w;
+      if (s_max[s] >= s_min[s]) w += ((s_max[s] - s_min[s]) >> 5) + 1;
+      if (w > kBitmapWords) { s_fail = 1; break; }
+    }
+    s_wbase[nslots] = (unsigned)w;
+    s_total_words = (unsigned)w;
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (threadIdx.x == 0) fb_list[atomicAdd(fb_count, 1u)] = b;
+    return;
+  }
+  const unsigned W = s_total_words;
+  for (unsigned w = threadIdx.x; w < W; w += blockDim.x) bm[w] = 0u;
+  __syncthreads();
+  for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const RankRec r = recs[r0 + i];
+    const int s = (int)(((long long)r.bin - bmin) >> logNB);
+    const unsigned pos = r.code - s_min[s];
+    atomicOr(&bm[s_wbase[s] + (pos >> 5)], 1u << (pos & 31));
+  }
+  __syncthreads();
+  // exclusive prefix popcount over the bitmap words (each thread owns a run)
+  {
+    const unsigned per = (W + blockDim.x - 1) / blockDim.x;
+    const unsigned w0 = threadIdx.x * per;
+    unsigned s = 0;
+    for (unsigned i = 0; i < per; i++) if (w0 + i < W) s += __popc(bm[w0 + i]);
+    __shared__ unsigned part[kRankThreads];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+      unsigned v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0u;
+      __syncthreads();
+      part[threadIdx.x] += v;
+      __syncthreads();
+    }
+    unsigned run = part[threadIdx.x] - s;
+    for (unsigned i = 0; i < per; i++)
+      if (w0 + i < W) { pref[w0 + i] = run; run += __popc(bm[w0 + i]); }
+  }
+  __syncthreads();
+  for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const RankRec r = recs[r0 + i];
+    if (r.dest == kNoExtremum) continue;
+    const int s = (int)(((long long)r.bin - bmin) >> logNB);
+    const unsigned pos = r.code - s_min[s];
+    const unsigned w = s_wbase[s] + (pos >> 5);
+    const unsigned below = __popc(bm[w] & ((1u << (pos & 31)) - 1u));
+    out[r.dest] = (int)(pref[w] - pref[s_wbase[s]] + below);
+  }
+}
+
+// ---- 3. fallback: device-wide LSD radix sort on (bin, code) ---------------
+// gather the records of the failed buckets into a contiguous list
+__global__ void fb_gather_count_kernel(const unsigned *__restrict__ fb_list, unsigned nfb,
+                                       const unsigned long long *__restrict__ start,
+                                       unsigned long long *__restrict__ fb_len) {
+  unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nfb) fb_len[i] = start[fb_list[i] + 1] - start[fb_list[i]];
+}
+
+__global__ void fb_gather_kernel(const unsigned *__restrict__ fb_list, unsigned nfb,
+                                 const unsigned long long *__restrict__ start,
+                                 const unsigned long long *__restrict__ fb_off,
+                                 const RankRec *__restrict__ recs,
+                                 unsigned long long *__restrict__ key,
+                                 unsigned *__restrict__ val) {
+  for (unsigned f = blockIdx.x; f < nfb; f += gridDim.x) {
+    const unsigned long long r0 = start[fb_list[f]], r1 = start[fb_list[f] + 1];
+    const unsigned long long o = fb_off[f];
+    for (unsigned long long i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const RankRec r = recs[i];
+      key[o + (i - r0)] = ((unsigned long long)((unsigned)r.bin ^ 0x80000000u) << 32) | r.code;
+      val[o + (i - r0)] = r.dest;
+    }
+  }
+}
+
+constexpr int kRadixTile = 2048;   // items per tile (8 per thread)
+
+__global__ void radix_hist_kernel(const unsigned long long *__restrict__ key, unsigned long long n,
+                                  int shift, unsigned *__restrict__ H, unsigned ntiles) {
+  __shared__ unsigned h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * kRadixTile;
+  for (int i = threadIdx.x; i < kRadixTile; i += 256) {
+    const unsigned long long k = t0 + i;
+    if (k < n) atomicAdd(&h[(key[k] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  H[(size_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];  // digit-major
+}
+
+// exclusive scan of a u32 array in place (single CTA, used for small matrices)
+__global__ void scan_inplace_kernel(unsigned *__restrict__ a, unsigned long long n) {
+  __shared__ unsigned long long part[1024];
+  const unsigned long long per = (n + blockDim.x - 1) / blockDim.x;
+  const unsigned long long i0 = threadIdx.x * per;
+  unsigned long long s = 0;
+  for (unsigned long long i = 0; i < per; i++) if (i0 + i < n) s += a[i0 + i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+    unsigned long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  unsigned long long run = part[threadIdx.x] - s;
+  for (unsigned long long i = 0; i < per; i++)
+    if (i0 + i < n) { const unsigned v = a[i0 + i]; a[i0 + i] = (unsigned)run; run += v; }
+}
+
+// stable scatter: items of a tile are ranked in order, 256 at a time
+__global__ void radix_scatter_kernel(const unsigned long long *__restrict__ key,
+                                     const unsigned *__restrict__ val, unsigned long long n,
+                                     int shift, const unsigned *__restrict__ H, unsigned ntiles,
+                                     unsigned long long *__restrict__ key2,
+                                     unsigned *__restrict__ val2) {
+  __shared__ unsigned base[256];
+  __shared__ unsigned wcnt[8][256];
+  base[threadIdx.x] = H[(size_t)threadIdx.x * ntiles + blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned long long t0 = (unsigned long long)blockIdx.x * kRadixTile;
+  for (int c = 0; c < kRadixTile; c += 256) {
+    for (int w = 0; w < 8; w++) wcnt[w][threadIdx.x] = 0;
+    __syncthreads();
+    const unsigned long long k = t0 + c + threadIdx.x;
+    const bool in = k < n;
+    unsigned long long kv = in ? key[k] : 0ull;
+    const unsigned d = in ? (unsigned)((kv >> shift) & 255u) : 256u + (unsigned)warp;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const unsigned rank_in_warp = __popc(peers & ((1u << lane) - 1u));
+    const int leader = __ffs(peers) - 1;
+    if (in && lane == leader) wcnt[warp][d] = __popc(peers);
+    __syncthreads();
+    unsigned before = 0;
+    if (in) {
+      for (int w = 0; w < warp; w++) before += wcnt[w][d];
+      const unsigned pos = base[d] + before + rank_in_warp;
+      key2[pos] = kv;
+      val2[pos] = val[k];
+    }
+    __syncthreads();
+    // advance the per-digit base by this chunk's totals
+    unsigned tot = 0;
+    for (int w = 0; w < 8; w++) tot += wcnt[w][threadIdx.x];
+    base[threadIdx.x] += tot;
+    __syncthreads();
+  }
+}
+
+// dense rank inside bins of the sorted fallback list (one CTA, sequential chunks)
+__global__ void fb_rank_kernel(const unsigned long long *__restrict__ key,
+                               const unsigned *__restrict__ val, unsigned long long n,
+                               int *__restrict__ out) {
+  __shared__ int carry_rank;
+  __shared__ int wsum[8];
+  __shared__ long long wlast_binstart[8];
+  if (threadIdx.x == 0) carry_rank = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (unsigned long long c = 0; c < n; c += blockDim.x) {
+    const unsigned long long i = c + threadIdx.x;
+    const bool in = i < n;
+    const unsigned long long k = in ? key[i] : 0ull;
+    const unsigned long long kp = (in && i > 0) ? key[i - 1] : k;
+    const bool newbin = in && (i == 0 || (k >> 32) != (kp >> 32));
+    const int inc = (in && i > 0 && !newbin && (unsigned)k != (unsigned)kp) ? 1 : 0;
+    // segmented inclusive scan of inc, segments start at newbin
+    int v = inc;
+    bool seg = newbin;
+    for (int o = 1; o < 32; o <<= 1) {
+      int tv = __shfl_up_sync(0xffffffffu, v, o);
+      bool ts = __shfl_up_sync(0xffffffffu, seg, o);
+      if (lane >= o && !seg) { v += tv; seg = ts; }
+    }
+    if (lane == 31) { wsum[warp] = v; wlast_binstart[warp] = seg ? 1 : 0; }
+    __syncthreads();
+    // combine warps sequentially (8 warps)
+    int pre = 0;
+    bool cut = false;
+    for (int w = warp - 1; w >= 0 && !cut; w--) {
+      pre += wsum[w];
+      if (wlast_binstart[w]) cut = true;
+    }
+    int rank;
+    if (seg) rank = v;                     // a bin started inside this warp before/at me
+    else if (cut) rank = v + pre;          // a bin started in an earlier warp of this chunk
+    else rank = v + pre + carry_rank;      // bin continues from the previous chunk
+    if (in && val[i] != kNoExtremum) out[val[i]] = rank;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1 || i == n - 1) {
+      if (in) carry_rank = rank;
+    }
+    __syncthreads();
+  }
+}
+
+int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
+                   unsigned long long K, unsigned long long E, float eb, int *d_sp) {
+  if (K == 0) return 0;
+  cudaStream_t s = ctx->stream;
+  const double inv = 1.0 / (double)eb;
+  int logNB = 6;
+  while (logNB < 14 && (K >> logNB) > 2048) logNB++;
+  const int NB = 1 << logNB;
+  int G = ctx->sm_count * 2;
+  unsigned long long chunk = (K + G - 1) / G;
+  if (chunk < 4096) { chunk = 4096; G = (int)((K + chunk - 1) / chunk); }
+  Arena &A = ctx->scratch;
+  unsigned *M = A.take<unsigned>((size_t)G * NB);
+  unsigned *tot = A.take<unsigned>(NB);
+  unsigned long long *start = A.take<unsigned long long>(NB + 1);
+  RankRec *recs = A.take<RankRec>(K);
+  unsigned *fb_list = A.take<unsigned>(NB);
+  unsigned *fb_cnt = A.take<unsigned>(4);
+  if (!M || !tot || !start || !recs || !fb_list || !fb_cnt) {
+    set_error("scratch arena too small for the rank stage");
+    return -1;
+  }
+  const size_t hsm = (size_t)NB * 4;
+  cudaFuncSetAttribute(bucket_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm);
+  cudaFuncSetAttribute(bucket_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm);
+  bucket_hist_kernel<<<G, 512, hsm, s>>>(d_pairs, d_bins, K, eb, inv, logNB, chunk, M);
+  bucket_colscan_kernel<<<(NB + 255) / 256, 256, 0, s>>>(M, G, NB, tot);
+  bucket_start_kernel<<<1, 1024, 0, s>>>(tot, NB, start);
+  bucket_scatter_kernel<<<G, 512, hsm, s>>>(d_pairs, d_bins, K, eb, inv, logNB, chunk, M, start, recs);
+  if (cuda_fail(cudaMemsetAsync(fb_cnt, 0, 16, s), "memset")) return -1;
+  bucket_rank_kernel<<<NB, kRankThreads, 0, s>>>(recs, start, logNB, d_sp, fb_list, fb_cnt);
+  ctx->launches += 5;
+  if (cuda_fail(cudaGetLastError(), "rank kernels")) return -1;
+  unsigned nfb = 0;
+  if (cuda_fail(cudaMemcpyAsync(&nfb, fb_cnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaStreamSynchronize(s), "rank"))
+    return -1;
+  if (nfb == 0) return 0;
+
+  // ---- fallback ----
+  unsigned long long *fb_len = A.take<unsigned long long>(nfb + 1);
+  if (!fb_len) { set_error("scratch arena too small for the rank fallback"); return -1; }
+  fb_gather_count_kernel<<<(nfb + 255) / 256, 256, 0, s>>>(fb_list, nfb, start, fb_len);
+  std::vector<unsigned long long> h_len(nfb);
+  if (cuda_fail(cudaMemcpyAsync(h_len.data(), fb_len, nfb * 8, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaStreamSynchronize(s), "fallback"))
+    return -1;
+  std::vector<unsigned long long> h_off(nfb);
+  unsigned long long nf = 0;
+  for (unsigned i = 0; i < nfb; i++) { h_off[i] = nf; nf += h_len[i]; }
+  unsigned long long *fb_off = A.take<unsigned long long>(nfb);
+  unsigned long long *k1 = A.take<unsigned long long>(nf), *k2 = A.take<unsigned long long>(nf);
+  unsigned *v1 = A.take<unsigned>(nf), *v2 = A.take<unsigned>(nf);
+  const unsigned ntiles = (unsigned)((nf + kRadixTile - 1) / kRadixTile);
+  unsigned *H = A.take<unsigned>((size_t)256 * ntiles);
+  if (!fb_off || !k1 || !k2 || !v1 || !v2 || !H) {
+    set_error("scratch arena too small for the rank fallback");
+    return -1;
+  }
+  cudaMemcpyAsync(fb_off, h_off.data(), nfb * 8, cudaMemcpyHostToDevice, s);
+  fb_gather_kernel<<<std::min(nfb, 4096u), 256, 0, s>>>(fb_list, nfb, start, fb_off, recs, k1, v1);
+  for (int shift = 0; shift < 64; shift += 8) {
+    radix_hist_kernel<<<ntiles, 256, 0, s>>>(k1, nf, shift, H, ntiles);
+    scan_inplace_kernel<<<1, 1024, 0, s>>>(H, (unsigned long long)256 * ntiles);
+    radix_scatter_kernel<<<ntiles, 256, 0, s>>>(k1, v1, nf, shift, H, ntiles, k2, v2);
+    std::swap(k1, k2);
+    std::swap(v1, v2);
+  }
+  fb_rank_kernel<<<1, 256, 0, s>>>(k1, v1, nf, d_sp);
+  ctx->launches += 3 + 8 * 3;
+  if (cuda_fail(cudaGetLastError(), "fallback kernels") ||
+      cuda_fail(cudaStreamSynchronize(s), "fallback"))
+    return -1;
+  (void)E;
+  return 0;
+}
+
+size_t rank_scratch_bytes(unsigned long long K, int sm_count) {
+  int logNB = 6;
+  while (logNB < 14 && (K >> logNB) > 2048) logNB++;
+  const size_t NB = (size_t)1 << logNB;
+  const size_t G = (size_t)sm_count * 2 + 1;
+  // fallback worst case: all K records (two key/value ping-pong buffers + histogram)
+  const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4);
+  return a256(G * NB * 4) + a256(NB * 4) + a256((NB + 1) * 8) + a256(K * sizeof(RankRec)) +
+         a256(NB * 4) * 2 + a256(16) + fb + 4096;
+}
+
+// ---------------------------------------------------------------------------
+// extrema compaction in list order (for the reference's sort-position
+// compression of an arbitrary CP list, SZp/src/szp_cuda_topology.cu:436-449)
+// ---------------------------------------------------------------------------
+__global__ void extrema_compact_kernel(const int *__restrict__ cps, int stride, int type_field,
+                                       unsigned long long K, TileDesc *desc, unsigned *tile_ctr,
+                                       int *err, int *__restrict__ sp,
+                                       unsigned long long *__restrict__ total) {
+  __shared__ long long s_tile;
+  __shared__ unsigned s_w[8];
+  __shared__ unsigned long long s_base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int T = 2048;
+  const long long ntiles = (long long)((K + T - 1) / T);
+  while (true) {
+    if (threadIdx.x == 0) s_tile = (long long)atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= ntiles) break;
+    // each thread owns 8 consecutive items
+    const unsigned long long i0 = (unsigned long long)tile * T + threadIdx.x * 8;
+    unsigned flags = 0, c = 0;
+    for (int u = 0; u < 8; u++) {
+      const unsigned long long i = i0 + u;
+      if (i < K) {
+        const int t = cps[(size_t)i * stride + type_field];
+        if (t == 1 || t == 2) { flags |= 1u << u; c++; }
+      }
+    }
+    unsigned incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    unsigned wpre = 0, ttot = 0;
+    for (int w = 0; w < 8; w++) { if (w < warp) wpre += s_w[w]; ttot += s_w[w]; }
+    if (warp == 0) {
+      Prefix pf = lookback(desc, tile, 0, ttot, err);
+      if (lane == 0) {
+        s_base = pf.cnt;
+        if (tile == ntiles - 1) *total = pf.cnt + ttot;
+      }
+    }
+    __syncthreads();
+    unsigned long long o = s_base + wpre + incl - c;
+    for (int u = 0; u < 8; u++)
+      if (flags & (1u << u)) sp[o++] = cps[(size_t)(i0 + u) * stride + 4 + (stride == 6 ? 1 : 0)];
+    __syncthreads();
+  }
+}
+
+int compact_extrema(szp_b200_ctx *ctx, const int *d_cps, int stride, unsigned long long K,
+                    int *d_sp, unsigned long long *E_out) {
+  cudaStream_t s = ctx->stream;
+  const unsigned long long ntiles = (K + 2047) / 2048;
+  TileDesc *desc = ctx->scratch.take<TileDesc>(ntiles + 1);
+  if (!desc) { set_error("scratch arena too small"); return -1; }
+  unsigned long long *w = ctx->d_words;
+  if (cuda_fail(cudaMemsetAsync(desc, 0, (ntiles + 1) * sizeof(TileDesc), s), "memset") ||
+      cuda_fail(cudaMemsetAsync(w, 0, 64, s), "memset"))
+    return -1;
+  const int grid = (int)std::min<unsigned long long>(ntiles, (unsigned long long)ctx->sm_count * 8);
+  extrema_compact_kernel<<<grid, 256, 0, s>>>(d_cps, stride, stride == 6 ? 3 : 2, K, desc,
+                                              reinterpret_cast<unsigned *>(w + 3),
+                                              reinterpret_cast<int *>(w + 4), d_sp, w);
+  ctx->launches += 1;
+  if (cuda_fail(cudaGetLastError(), "compact") ||
+      cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 64, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaStreamSynchronize(s), "compact"))
+    return -1;
+  if (ctx->h_words[4] & 0xffffffffu) { set_error("compaction status %d", (int)ctx->h_words[4]); return -1; }
+  *E_out = ctx->h_words[0];
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// API sort of an arbitrary CP list: every CP gets its rank
+// ---------------------------------------------------------------------------
+__global__ void cp_pairs_kernel(const int *__restrict__ cps, int stride, unsigned long long K,
+                                const float *__restrict__ data, long long d2, long long d3,
+                                uint2 *__restrict__ pairs, int *__restrict__ bins) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= K) return;
+  const int *r = cps + (size_t)i * stride;
+  unsigned long long flat;
+  int bin;
+  if (stride == 5) { flat = (unsigned long long)(long long)r[0] * d3 + (long long)r[1]; bin = r[3]; }
+  else {
+    flat = (unsigned long long)(long long)r[0] * d2 * d3 + (unsigned long long)((long long)r[1] * d3) +
+           (long long)r[2];
+    bin = r[4];
+  }
+  pairs[i] = make_uint2(float_code(data[flat]), (unsigned)i);
+  bins[i] = bin;
+}
+
+__global__ void cp_store_rank_kernel(int *__restrict__ cps, int stride, unsigned long long K,
+                                     const int *__restrict__ rank) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < K) cps[(size_t)i * stride + stride - 1] = rank[i];
+}
+
+int sort_cp_list_host(int *h_cps, int stride, unsigned long long K, const float *h_data,
+                      long long d2, long long d3) {
+  szp_b200_ctx *ctx = default_ctx();
+  if (!ctx) return -1;
+  // extent of the data the list refers to (the reference copies data[0..max_flat])
+  unsigned long long max_flat = 0;
+  for (unsigned long long i = 0; i < K; i++) {
+    const int *r = h_cps + (size_t)i * stride;
+    unsigned long long f = (stride == 5)
+                               ? (unsigned long long)((long long)r[0] * d3 + r[1])
+                               : (unsigned long long)((long long)r[0] * d2 * d3 + (long long)r[1] * d3 + r[2]);
+    if (f > max_flat) max_flat = f;
+  }
+  if (max_flat >= (1ull << 40)) { set_error("critical point coordinates out of range"); return -1; }
+  const size_t need = a256((max_flat + 1) * 4) + a256(K * stride * 4) + a256(K * 8) + a256(K * 4) * 2 +
+                      rank_scratch_bytes(K, ctx->sm_count);
+  if (!ctx->scratch.reserve(need)) return -1;
+  Arena &A = ctx->scratch;
+  float *d_data = A.take<float>(max_flat + 1);
+  int *d_cps = A.take<int>(K * stride);
+  uint2 *d_pairs = A.take<uint2>(K);
+  int *d_bins = A.take<int>(K);
+  int *d_rank = A.take<int>(K);
+  cudaStream_t s = ctx->stream;
+  if (cuda_fail(cudaMemcpyAsync(d_data, h_data, (max_flat + 1) * 4, cudaMemcpyHostToDevice, s), "H2D") ||
+      cuda_fail(cudaMemcpyAsync(d_cps, h_cps, K * stride * 4, cudaMemcpyHostToDevice, s), "H2D"))
+    return -1;
+  const unsigned blocks = (unsigned)((K + 255) / 256);
+  cp_pairs_kernel<<<blocks, 256, 0, s>>>(d_cps, stride, K, d_data, d2, d3, d_pairs, d_bins);
+  if (rank_positions(ctx, d_pairs, d_bins, K, K, 1.0f, d_rank)) return -1;
+  cp_store_rank_kernel<<<blocks, 256, 0, s>>>(d_cps, stride, K, d_rank);
+  ctx->launches += 2;
+  if (cuda_fail(cudaMemcpyAsync(h_cps, d_cps, K * stride * 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaStreamSynchronize(s), "sort"))
+    return -1;
+  return 0;
+}
+
+}  // namespace tsz
+
+extern "C" {
+
+void szp_cuda_sort_critical_points_by_original_data(CriticalPoint *critical_points,
+                                                     size_t critical_count, float *data, int cols) {
+  tsz::clear_error();
+  if (!critical_points || critical_count == 0 || !data) return;
+  tsz::sort_cp_list_host(reinterpret_cast<int *>(critical_points), 5, critical_count, data, 1, cols);
+}
+
+void szp_cuda_sort_critical_points_3d(CriticalPoint3D *critical_points, size_t critical_count,
+                                      float *data, int d2, int d3) {
+  tsz::clear_error();
+  if (!critical_points || critical_count == 0 || !data) return;
+  tsz::sort_cp_list_host(reinterpret_cast<int *>(critical_points), 6, critical_count, data, d2, d3);
+}
+
+}  // extern "C"

@@ -1,0 +1,338 @@
+"""Python binding of libtoposzp_b200.so (the B200 topology path).
+
+Mirrors the reference's CUDA topology interface (SZp/include/szp_cuda_topology.cuh,
+szp_cuda_topology_3d.cuh, szp_cuda_decompress.cuh): the same entry points, the
+same argument meaning, the same CriticalPoint layouts and compressed bytes.
+The device-pointer functions take torch CUDA tensors.
+
+The library is required: importing this module on a machine without the
+built library raises, there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtoposzp_b200.so")
+
+CP2_DT = np.dtype([("x", "<i4"), ("y", "<i4"), ("type", "<i4"),
+                   ("quantized_bin", "<i4"), ("sort_position", "<i4")])
+CP3_DT = np.dtype([("x", "<i4"), ("y", "<i4"), ("z", "<i4"), ("type", "<i4"),
+                   ("quantized_bin", "<i4"), ("sort_position", "<i4")])
+
+EXPORTS = [
+    "szp_cuda_find_critical_points",
+    "szp_cuda_sort_critical_points_by_original_data",
+    "szp_cuda_compress_sort_positions",
+    "szp_cuda_float_compress_randomaccess_topology_preserved",
+    "szp_cuda_find_critical_points_3d",
+    "szp_cuda_sort_critical_points_3d",
+    "szp_cuda_compress_sort_positions_3d",
+    "szp_cuda_float_compress_topology_3d",
+    "szp_cuda_float_decompress_randomaccess_topology_preserved",
+    "szp_cuda_decompress_sort_positions",
+    "szp_b200_last_error",
+    "szp_b200_version",
+    "szp_b200_ctx_create",
+    "szp_b200_ctx_destroy",
+    "szp_b200_topo_bound",
+    "szp_b200_sort_bound",
+    "szp_b200_topo_compress_dev",
+    "szp_b200_topo_decompress_dev",
+    "szp_b200_topo_postprocess_dev",
+    "szp_b200_ctx_stage_times",
+    "szp_b200_ctx_launches",
+    "szp_b200_topo_compress_host",
+    "szp_b200_topo_decompress_host",
+]
+
+
+class ToposzpError(RuntimeError):
+    pass
+
+
+class Geom(C.Structure):
+    _fields_ = [("nd", C.c_int), ("dims", C.c_int * 3)]
+
+
+class Sizes(C.Structure):
+    _fields_ = [("topo_bytes", C.c_size_t), ("sort_bytes", C.c_size_t),
+                ("cp_count", C.c_size_t), ("extrema_count", C.c_size_t)]
+
+
+def build() -> str:
+    """Compile the library in place (nvcc, sm_100a)."""
+    subprocess.run(["make", "-s", "-C", HERE, "-j8"], check=True)
+    return LIB_PATH
+
+
+_lib = None
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ToposzpError("libtoposzp_b200.so is not built (run build())")
+        L = C.CDLL(LIB_PATH)
+        vp, sz, i, f = C.c_void_p, C.c_size_t, C.c_int, C.c_float
+        sig = {
+            "szp_cuda_find_critical_points": (vp, [vp, C.POINTER(sz), i, i, f]),
+            "szp_cuda_find_critical_points_3d": (vp, [vp, C.POINTER(sz), i, i, i, f]),
+            "szp_cuda_sort_critical_points_by_original_data": (None, [vp, sz, vp, i]),
+            "szp_cuda_sort_critical_points_3d": (None, [vp, sz, vp, i, i]),
+            "szp_cuda_compress_sort_positions": (vp, [vp, sz, C.POINTER(sz), i]),
+            "szp_cuda_compress_sort_positions_3d": (vp, [vp, sz, C.POINTER(sz), i]),
+            "szp_cuda_float_compress_randomaccess_topology_preserved":
+                (vp, [vp, C.POINTER(sz), f, sz, i, vp, i, i, i]),
+            "szp_cuda_float_compress_topology_3d": (vp, [vp, C.POINTER(sz), f, sz, i, vp, i, i, i, i]),
+            "szp_cuda_float_decompress_randomaccess_topology_preserved":
+                (None, [C.POINTER(vp), sz, f, i, vp, C.POINTER(vp)]),
+            "szp_cuda_decompress_sort_positions": (vp, [vp, sz, i]),
+            "szp_b200_last_error": (C.c_char_p, []),
+            "szp_b200_version": (C.c_char_p, []),
+            "szp_b200_ctx_create": (vp, [vp]),
+            "szp_b200_ctx_destroy": (None, [vp]),
+            "szp_b200_topo_bound": (sz, [sz, i]),
+            "szp_b200_sort_bound": (sz, [sz, i]),
+            "szp_b200_topo_compress_dev": (i, [vp, vp, Geom, f, i, vp, vp, vp, C.POINTER(Sizes)]),
+            "szp_b200_topo_decompress_dev": (i, [vp, vp, sz, vp, sz, vp, Geom, f, i, vp, vp, i]),
+            "szp_b200_topo_postprocess_dev": (i, [vp, vp, vp, vp, vp, sz, Geom, f, i]),
+            "szp_b200_ctx_stage_times": (i, [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_float), i]),
+            "szp_b200_ctx_launches": (C.c_ulonglong, [vp]),
+            "szp_b200_topo_compress_host": (i, [vp, vp, Geom, f, i, vp, sz, vp, sz, C.POINTER(Sizes)]),
+            "szp_b200_topo_decompress_host": (i, [vp, vp, sz, vp, sz, Geom, f, i, vp, i]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().szp_b200_last_error().decode()
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _take(ptr, nbytes, dtype):
+    if not ptr:
+        return None
+    buf = (C.c_char * nbytes).from_address(ptr)
+    out = np.frombuffer(bytes(buf), dtype=dtype).copy()
+    _libc.free(ptr)
+    return out
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ---------------------------------------------------------------------------
+# reference entry points (host buffers)
+# ---------------------------------------------------------------------------
+
+def find_critical_points(data: np.ndarray, eb: float) -> np.ndarray:
+    """szp_cuda_find_critical_points[_3d]: CPs in raster order."""
+    d = _f32(data)
+    k = C.c_size_t(0)
+    if d.ndim == 2:
+        ptr = lib().szp_cuda_find_critical_points(_p(d), C.byref(k), d.shape[0], d.shape[1], eb)
+        dt = CP2_DT
+    else:
+        ptr = lib().szp_cuda_find_critical_points_3d(_p(d), C.byref(k), *d.shape, eb)
+        dt = CP3_DT
+    if not ptr:
+        err = last_error()
+        if err:
+            raise ToposzpError(err)
+        return np.zeros(0, dtype=dt)
+    return _take(ptr, k.value * dt.itemsize, dt)
+
+
+def sort_critical_points(cps: np.ndarray, data: np.ndarray) -> np.ndarray:
+    """szp_cuda_sort_critical_points_by_original_data / _3d (returns a sorted copy)."""
+    cp = np.ascontiguousarray(cps).copy()
+    d = _f32(data)
+    if len(cp) == 0:
+        return cp
+    if cp.dtype == CP2_DT:
+        lib().szp_cuda_sort_critical_points_by_original_data(_p(cp), len(cp), _p(d), d.shape[-1])
+    else:
+        lib().szp_cuda_sort_critical_points_3d(_p(cp), len(cp), _p(d), d.shape[1], d.shape[2])
+    err = last_error()
+    if err:
+        raise ToposzpError(err)
+    return cp
+
+
+def compress_sort_positions(cps: np.ndarray, block_size: int) -> bytes:
+    cp = np.ascontiguousarray(cps)
+    sz = C.c_size_t(0)
+    if cp.dtype == CP2_DT:
+        ptr = lib().szp_cuda_compress_sort_positions(_p(cp), len(cp), C.byref(sz), block_size)
+    else:
+        ptr = lib().szp_cuda_compress_sort_positions_3d(_p(cp), len(cp), C.byref(sz), block_size)
+    if not ptr:
+        err = last_error()
+        if err:
+            raise ToposzpError(err)
+        return b""
+    return _take(ptr, sz.value, np.uint8).tobytes()
+
+
+def compress_topology(data: np.ndarray, eb: float, block_size: int, cps: np.ndarray) -> bytes:
+    """szp_cuda_float_compress_randomaccess_topology_preserved (2D) or
+    szp_cuda_float_compress_topology_3d (3D)."""
+    d = _f32(data)
+    cp = np.ascontiguousarray(cps)
+    sz = C.c_size_t(0)
+    if d.ndim == 2:
+        ptr = lib().szp_cuda_float_compress_randomaccess_topology_preserved(
+            _p(d), C.byref(sz), eb, d.size, block_size, _p(cp) if len(cp) else None, len(cp),
+            d.shape[0], d.shape[1])
+    else:
+        ptr = lib().szp_cuda_float_compress_topology_3d(
+            _p(d), C.byref(sz), eb, d.size, block_size, _p(cp) if len(cp) else None, len(cp),
+            *d.shape)
+    if not ptr:
+        raise ToposzpError(last_error() or "compression returned NULL")
+    return _take(ptr, sz.value, np.uint8).tobytes()
+
+
+def decompress_topology(stream: bytes, n: int, eb: float, block_size: int):
+    """szp_cuda_float_decompress_randomaccess_topology_preserved -> (data, FN)."""
+    s = np.frombuffer(stream, dtype=np.uint8)
+    outp, fnp = C.c_void_p(), C.c_void_p()
+    lib().szp_cuda_float_decompress_randomaccess_topology_preserved(
+        C.byref(outp), n, eb, block_size, _p(s), C.byref(fnp))
+    if not outp.value:
+        raise ToposzpError(last_error() or "decompression returned NULL")
+    return _take(outp.value, 4 * n, np.float32), _take(fnp.value, 4 * n, np.int32)
+
+
+def decompress_sort_positions(stream: bytes, count: int, block_size: int) -> np.ndarray:
+    s = np.frombuffer(stream, dtype=np.uint8)
+    ptr = lib().szp_cuda_decompress_sort_positions(_p(s), count, block_size)
+    if not ptr:
+        raise ToposzpError(last_error() or "sort-position decompression returned NULL")
+    return _take(ptr, 4 * count, np.int32)
+
+
+# ---------------------------------------------------------------------------
+# device-pointer entry points (torch CUDA tensors)
+# ---------------------------------------------------------------------------
+
+def geom_of(shape) -> Geom:
+    g = Geom()
+    g.nd = len(shape)
+    for i, v in enumerate(shape):
+        g.dims[i] = int(v)
+    return g
+
+
+class Context:
+    """A reusable device workspace bound to a CUDA stream (0 = own stream)."""
+
+    def __init__(self, stream_handle: int = 0):
+        self.ptr = lib().szp_b200_ctx_create(C.c_void_p(stream_handle) if stream_handle else None)
+        if not self.ptr:
+            raise ToposzpError(last_error())
+
+    def close(self):
+        if self.ptr:
+            lib().szp_b200_ctx_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compress(self, d_data, shape, eb: float, block_size: int = 64, index=True):
+        """Fused compression of a device field -> (topo, sort, index, sizes).
+        topo / sort are uint8 device tensors sized to the streams."""
+        import torch
+        n = int(np.prod(shape))
+        L = lib()
+        topo = torch.empty(L.szp_b200_topo_bound(n, block_size), dtype=torch.uint8, device=d_data.device)
+        sort = torch.empty(L.szp_b200_sort_bound(n, block_size), dtype=torch.uint8, device=d_data.device)
+        nb = (n + block_size - 1) // block_size
+        idx = torch.empty(2 * nb, dtype=torch.int64, device=d_data.device) if index else None
+        sizes = Sizes()
+        rc = L.szp_b200_topo_compress_dev(
+            self.ptr, C.c_void_p(d_data.data_ptr()), geom_of(shape), eb, block_size,
+            C.c_void_p(topo.data_ptr()), C.c_void_p(sort.data_ptr()),
+            C.c_void_p(idx.data_ptr()) if idx is not None else None, C.byref(sizes))
+        if rc:
+            raise ToposzpError(last_error())
+        return topo, sort, idx, sizes
+
+    def decompress(self, topo, topo_bytes, sort, sort_bytes, index, shape, eb: float,
+                   block_size: int = 64, postprocess: int = 1, out=None, types=None):
+        import torch
+        n = int(np.prod(shape))
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device=topo.device)
+        rc = lib().szp_b200_topo_decompress_dev(
+            self.ptr, C.c_void_p(topo.data_ptr()), topo_bytes,
+            C.c_void_p(sort.data_ptr()) if sort is not None else None, sort_bytes,
+            C.c_void_p(index.data_ptr()), geom_of(shape), eb, block_size,
+            C.c_void_p(out.data_ptr()), C.c_void_p(types.data_ptr()) if types is not None else None,
+            postprocess)
+        if rc:
+            raise ToposzpError(last_error())
+        return out
+
+    def stage_times(self):
+        """[(stage, ms)] of the last call, from CUDA events on the workspace stream."""
+        names = (C.c_char_p * 24)()
+        ms = (C.c_float * 24)()
+        k = lib().szp_b200_ctx_stage_times(self.ptr, names, ms, 24)
+        return [(names[i].decode(), float(ms[i])) for i in range(k)]
+
+    def launches(self) -> int:
+        return int(lib().szp_b200_ctx_launches(self.ptr))
+
+    def compress_host(self, h_data: np.ndarray, eb: float, block_size: int, h_topo: np.ndarray,
+                      h_sort: np.ndarray) -> Sizes:
+        """Host-buffer fused compression (h_* may be pinned numpy views)."""
+        sizes = Sizes()
+        rc = lib().szp_b200_topo_compress_host(
+            self.ptr, h_data.ctypes.data_as(C.c_void_p), geom_of(h_data.shape), eb, block_size,
+            h_topo.ctypes.data_as(C.c_void_p), h_topo.nbytes, h_sort.ctypes.data_as(C.c_void_p),
+            h_sort.nbytes, C.byref(sizes))
+        if rc:
+            raise ToposzpError(last_error())
+        return sizes
+
+    def decompress_host(self, h_topo: np.ndarray, topo_bytes: int, h_sort: np.ndarray, sort_bytes: int,
+                        shape, eb: float, block_size: int, h_out: np.ndarray, postprocess: int = 1):
+        rc = lib().szp_b200_topo_decompress_host(
+            self.ptr, h_topo.ctypes.data_as(C.c_void_p), topo_bytes,
+            h_sort.ctypes.data_as(C.c_void_p) if sort_bytes else None, sort_bytes, geom_of(shape), eb,
+            block_size, h_out.ctypes.data_as(C.c_void_p), postprocess)
+        if rc:
+            raise ToposzpError(last_error())
+        return h_out
+
+    def postprocess(self, d_data, d_orig, d_types_int, d_sp, shape, eb: float, axis_stencil=False):
+        rc = lib().szp_b200_topo_postprocess_dev(
+            self.ptr, C.c_void_p(d_data.data_ptr()), C.c_void_p(d_orig.data_ptr()),
+            C.c_void_p(d_types_int.data_ptr()),
+            C.c_void_p(d_sp.data_ptr()) if d_sp is not None and d_sp.numel() else None,
+            0 if d_sp is None else d_sp.numel(), geom_of(shape), eb, int(axis_stencil))
+        if rc:
+            raise ToposzpError(last_error())
+        return d_data
