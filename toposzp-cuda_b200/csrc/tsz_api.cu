@@ -62,7 +62,7 @@ int encode_pass(szp_b200_ctx *ctx, int mode, const float *d_data, const int *d_i
                 unsigned long long totals_out[3]) {
   cudaStream_t s = ctx->stream;
   const unsigned long long nb = (n + B - 1) / B;
-  const int TB = tile_blocks_for(B);
+  const int TB = enc_tile_blocks(B);
   const unsigned long long ntiles = (nb + TB - 1) / TB;
   TileDesc *desc = ctx->scratch.take<TileDesc>(ntiles + 1);
   if (!desc) { set_error("scratch arena too small for tile descriptors"); return -1; }
@@ -258,7 +258,7 @@ static unsigned char *compress_host_path(const char *fn, const float *h_data, si
   const size_t cps_bytes = (h_cps && count > 0) ? (size_t)count * stride * sizeof(int) : 0;
   const unsigned long long nb = (n + B - 1) / B;
   const size_t need = a256(n * 4) + a256(n) + a256(cap) + a256(cps_bytes) +
-                      a256((nb / tile_blocks_for(B) + 2) * sizeof(TileDesc)) + 4096;
+                      a256((nb / enc_tile_blocks(B) + 2) * sizeof(TileDesc)) + 4096;
   if (!ctx->scratch.reserve(need)) return nullptr;
   float *d_data = ctx->scratch.take<float>(n);
   unsigned char *d_types = ctx->scratch.take<unsigned char>(n);
@@ -308,7 +308,7 @@ static void *find_host_path(const float *h_data, size_t *outCount, int nd, long 
   const int B = 64;
   const unsigned long long nb = (n + B - 1) / B;
   const size_t need = a256(n * 4) + a256(interior * rec * 4) +
-                      a256((nb / tile_blocks_for(B) + 2) * sizeof(TileDesc)) + 4096;
+                      a256((nb / enc_tile_blocks(B) + 2) * sizeof(TileDesc)) + 4096;
   if (!ctx->scratch.reserve(need)) return nullptr;
   float *d_data = ctx->scratch.take<float>(n);
   int *d_rec = ctx->scratch.take<int>(interior * rec);
@@ -542,7 +542,7 @@ int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_data, szp_b200_
   const int B = blockSize;
   const unsigned long long nb = (n + B - 1) / B;
   const unsigned long long kcap = n;
-  const size_t need = a256(kcap * 8) + a256(n * 4) + a256((nb / tile_blocks_for(B) + 2) * sizeof(TileDesc)) * 2 +
+  const size_t need = a256(kcap * 8) + a256(n * 4) + a256((nb / enc_tile_blocks(B) + 2) * sizeof(TileDesc)) * 2 +
                       rank_scratch_bytes(kcap, ctx->sm_count) + 8192;
   if (!ctx->scratch.reserve(need)) return -1;
   Arena &A = ctx->scratch;
@@ -644,9 +644,10 @@ int szp_b200_topo_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_topo,
   unsigned long long *S = post_words(ctx, n);
   const unsigned long long ntiles = (n + 2047) / 2048;
   TileDesc *desc = A.take<TileDesc>(ntiles + 1);
-  if (!S || !desc) { set_error("scratch arena too small for post-processing"); return -1; }
+  unsigned *Lb = A.take<unsigned>((n + 31) / 32);
+  if (!S || !desc || !Lb) { set_error("scratch arena too small for post-processing"); return -1; }
   int restored = 0;
-  return postprocess_with(ctx, d_out, O, T, S, desc, spp, spp ? E : 0, g, absErrBound,
+  return postprocess_with(ctx, d_out, O, T, S, desc, Lb, spp, spp ? E : 0, g, absErrBound,
                           postprocess == 2, &restored);
 }
 
@@ -680,7 +681,7 @@ static unsigned char *compress_sp_host(const int *h_cps, int stride, size_t K, s
   const size_t cap = stream_bound(K, B, false);
   const size_t need = a256(K * stride * 4) + a256(K * 4) + a256(cap) +
                       a256((K / 2048 + 2) * sizeof(TileDesc)) +
-                      a256((K / B / tile_blocks_for(B) + 2) * sizeof(TileDesc)) + 8192;
+                      a256((K / B / enc_tile_blocks(B) + 2) * sizeof(TileDesc)) + 8192;
   if (!ctx->scratch.reserve(need)) return nullptr;
   Arena &A = ctx->scratch;
   int *d_cps = A.take<int>(K * stride);

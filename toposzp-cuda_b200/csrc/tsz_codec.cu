@@ -14,6 +14,7 @@
 //      its CP / extremum offsets; the tile image is then written out with
 //      aligned 32-bit stores (edge bytes stored individually).
 #include "tsz_codec.h"
+#include "tsz_codec2.cuh"
 #include "tsz_lookback.cuh"
 
 namespace tsz {
@@ -535,7 +536,49 @@ static cudaError_t launch_enc_mode(const EncArgs &a, cudaStream_t s, int grid) {
   }
 }
 
+// ---- octet kernels (blockSize <= 256) ----
+int octet_group(int B) {
+  const int o = (B + 7) / 8;
+  int g = 1;
+  while (g < o) g <<= 1;
+  return g;
+}
+
+size_t enc2_smem_bytes(int B, bool tags) {
+  const int tb = kWarps * (32 / octet_group(B));
+  return (((size_t)tb * max_block_bytes((uint32_t)B, tags) + 64) + 15) & ~(size_t)15;
+}
+
+template <int MODE, int G>
+static cudaError_t launch_enc2(const EncArgs &a, cudaStream_t s, int grid) {
+  auto k = encode2_kernel<MODE, G>;
+  const size_t sm = enc2_smem_bytes(a.B, MODE != kEncInts);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  k<<<grid, kThreads, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t launch_enc2_mode(const EncArgs &a, cudaStream_t s, int grid) {
+  switch (octet_group(a.B)) {
+    case 1: return launch_enc2<MODE, 1>(a, s, grid);
+    case 2: return launch_enc2<MODE, 2>(a, s, grid);
+    case 4: return launch_enc2<MODE, 4>(a, s, grid);
+    case 8: return launch_enc2<MODE, 8>(a, s, grid);
+    case 16: return launch_enc2<MODE, 16>(a, s, grid);
+    default: return launch_enc2<MODE, 32>(a, s, grid);
+  }
+}
+
+int enc_tile_blocks(int B) { return B <= 256 ? kWarps * (32 / octet_group(B)) : tile_blocks_for(B); }
+
 cudaError_t launch_encode(int mode, const EncArgs &a, cudaStream_t s, int grid) {
+  if (a.B <= 256) {
+    if (mode == kEncClassify) return launch_enc2_mode<kEncClassify>(a, s, grid);
+    if (mode == kEncTypes) return launch_enc2_mode<kEncTypes>(a, s, grid);
+    return launch_enc2_mode<kEncInts>(a, s, grid);
+  }
   if (mode == kEncClassify) return launch_enc_mode<kEncClassify>(a, s, grid);
   if (mode == kEncTypes) return launch_enc_mode<kEncTypes>(a, s, grid);
   return launch_enc_mode<kEncInts>(a, s, grid);
@@ -564,7 +607,35 @@ static cudaError_t launch_dec_tags(const DecArgs &a, cudaStream_t s) {
   }
 }
 
+template <bool TAGS, int G>
+static cudaError_t launch_dec2(DecArgs a, cudaStream_t s) {
+  auto k = decode2_kernel<TAGS, G>;
+  const int tb = kWarps * (32 / G);
+  const size_t sm = (((size_t)tb * max_block_bytes((uint32_t)a.B, TAGS) + 64) + 15) & ~(size_t)15;
+  a.img_cap = sm - 32;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  const long long nblocks = ((long long)a.n + a.B - 1) / a.B;
+  const long long tiles = (nblocks + tb - 1) / tb;
+  if (tiles <= 0) return cudaSuccess;
+  k<<<(unsigned)tiles, kThreads, sm, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <bool TAGS>
+static cudaError_t launch_dec2_tags(DecArgs a, cudaStream_t s) {
+  switch (octet_group(a.B)) {
+    case 1: return launch_dec2<TAGS, 1>(a, s);
+    case 2: return launch_dec2<TAGS, 2>(a, s);
+    case 4: return launch_dec2<TAGS, 4>(a, s);
+    case 8: return launch_dec2<TAGS, 8>(a, s);
+    case 16: return launch_dec2<TAGS, 16>(a, s);
+    default: return launch_dec2<TAGS, 32>(a, s);
+  }
+}
+
 cudaError_t launch_decode(bool tags, DecArgs a, cudaStream_t s) {
+  if (a.B <= 256) return tags ? launch_dec2_tags<true>(a, s) : launch_dec2_tags<false>(a, s);
   a.img_cap = dec_smem_bytes(a.B, tags) - 16;
   return tags ? launch_dec_tags<true>(a, s) : launch_dec_tags<false>(a, s);
 }

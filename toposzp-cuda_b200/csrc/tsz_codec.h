@@ -44,6 +44,7 @@ struct DecArgs {
   unsigned long long img_cap;   // set by the launcher
 };
 
+int enc_tile_blocks(int B);   // codec blocks per encoder tile (look-back granularity)
 int kmax_for(int B);
 int bpw_for(int kmax);
 int tile_blocks_for(int B);

@@ -1,0 +1,632 @@
+// Octet codec kernels (blockSize <= 256).
+//
+// Each lane owns 8 consecutive elements of a codec block ("octet" l covers
+// elements 8l..8l+7 and deltas 8l..8l+7); a group of G = next_pow2(ceil(B/8))
+// lanes serves one block, a warp serves 32/G blocks.  With this mapping every
+// section of the block layout is byte-aligned per lane: the 8 sign bits of an
+// octet are one byte, its 8 remainder fields are exactly `rem` bytes, its 8
+// tags are two bytes and its full magnitude bytes are contiguous.  Packing and
+// unpacking therefore need no cross-lane bit merging; the decoder's prefix
+// sum is an in-lane serial sum plus a log2(G) group scan.
+#pragma once
+#include "tsz_codec.h"
+#include "tsz_lookback.cuh"
+
+namespace tsz {
+
+// loads 8 floats at p[i..i+7]: one 32-byte vector load when aligned and fully
+// in range, otherwise scalar loads for the elements selected by need
+__device__ __forceinline__ void load_oct(const float *__restrict__ p, long long i, long long n,
+                                         unsigned need, float (&v)[8]) {
+  if (need == 0) return;
+  if (i >= 0 && i + 8 <= n && ((reinterpret_cast<uintptr_t>(p + i) & 15) == 0)) {
+    const float4 a = __ldg(reinterpret_cast<const float4 *>(p + i));
+    const float4 b = __ldg(reinterpret_cast<const float4 *>(p + i) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int t = 0; t < 8; t++)
+      if (need & (1u << t)) v[t] = __ldg(p + i + t);
+  }
+}
+
+// 2-bit types of an octet (element t in bits 2t..2t+1); c[] holds the values
+// of the octet, nv of them valid, i0 the flat index of element 0
+__device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, long long n, long long i0,
+                                                   int nv, const float (&c)[8], const Geom &g) {
+  // coordinates of element 0, then incremented with wrap-around
+  long long r, x, y, z;
+  if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
+  else { x = fdivmod(i0, g.plane, g.m_plane, r); y = fdivmod(r, g.d3, g.m_d3, z); }
+  unsigned inter = 0;
+#pragma unroll
+  for (int t = 0; t < 8; t++) {
+    const bool in = t < nv;
+    bool ok = in && y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
+    if (g.nd == 3) ok = ok && x >= 1 && x <= g.d1 - 2;
+    if (ok) inter |= 1u << t;
+    z++;
+    while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
+  }
+  if (inter == 0) return 0u;
+  // +-1 neighbours: inside the octet, plus one scalar load at each end
+  const float prev = (inter & 1u) ? __ldg(d + i0 - 1) : 0.f;
+  float next = 0.f;
+#pragma unroll
+  for (int t = 0; t < 8; t++)
+    if (t == nv - 1 && (inter & (1u << t))) next = __ldg(d + i0 + nv);
+  const long long o1 = (g.nd == 2) ? g.d3 : g.plane;  // first axis: rows (2D) or planes (3D)
+  unsigned all_gt = inter, all_lt = inter, any_hi = 0, any_lo = 0, hi_a = 0, lo_a = 0;
+  {
+    float m[8], p[8];
+    load_oct(d, i0 - o1, n, inter, m);
+    load_oct(d, i0 + o1, n, inter, p);
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      const unsigned b = 1u << t;
+      if (!(inter & b)) continue;
+      const bool gm = c[t] > m[t], gp = c[t] > p[t], lm = c[t] < m[t], lp = c[t] < p[t];
+      if (!(gm && gp)) all_gt &= ~b;
+      if (!(lm && lp)) all_lt &= ~b;
+      if (gm && gp) hi_a |= b;
+      if (lm && lp) lo_a |= b;
+    }
+  }
+  unsigned hi_b = 0, lo_b = 0;
+  if (g.nd == 3) {
+    float m[8], p[8];
+    load_oct(d, i0 - g.d3, n, inter, m);
+    load_oct(d, i0 + g.d3, n, inter, p);
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      const unsigned b = 1u << t;
+      if (!(inter & b)) continue;
+      const bool gm = c[t] > m[t], gp = c[t] > p[t], lm = c[t] < m[t], lp = c[t] < p[t];
+      if (!(gm && gp)) all_gt &= ~b;
+      if (!(lm && lp)) all_lt &= ~b;
+      if (gm && gp) hi_b |= b;
+      if (lm && lp) lo_b |= b;
+    }
+  }
+  unsigned hi_c = 0, lo_c = 0;
+#pragma unroll
+  for (int t = 0; t < 8; t++) {
+    const unsigned b = 1u << t;
+    if (!(inter & b)) continue;
+    const float lf = (t == 0) ? prev : c[t - 1 < 0 ? 0 : t - 1];
+    const float rt = (t == nv - 1) ? next : c[t + 1 > 7 ? 7 : t + 1];
+    const bool gm = c[t] > lf, gp = c[t] > rt, lm = c[t] < lf, lp = c[t] < rt;
+    if (!(gm && gp)) all_gt &= ~b;
+    if (!(lm && lp)) all_lt &= ~b;
+    if (gm && gp) hi_c |= b;
+    if (lm && lp) lo_c |= b;
+  }
+  const unsigned mx = all_gt, mn = all_lt & ~mx;
+  unsigned sd;
+  if (g.nd == 2) {
+    // vertical axis (rows) is a, horizontal (columns) is c
+    sd = ((lo_a & hi_c) | (hi_a & lo_c)) & ~mx & ~mn;
+  } else {
+    sd = (hi_a | hi_b | hi_c) & (lo_a | lo_b | lo_c) & ~mx & ~mn;
+  }
+  unsigned types = 0;
+#pragma unroll
+  for (int t = 0; t < 8; t++) {
+    const unsigned b = 1u << t;
+    const unsigned ty = (mx & b) ? 1u : (mn & b) ? 2u : (sd & b) ? 3u : 0u;
+    types |= ty << (2 * t);
+  }
+  return types;
+}
+
+// CTA-wide exclusive scan of one value per thread (kThreads threads);
+// returns the exclusive prefix and writes the total to *total
+__device__ __forceinline__ unsigned cta_excl_scan(unsigned v, unsigned *s_warp, unsigned *total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  unsigned wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; w++) {
+    const unsigned sw = s_warp[w];
+    if (w < warp) wpre += sw;
+    tot += sw;
+  }
+  *total = tot;
+  return wpre + inc - v;
+}
+
+template <int MODE, int G>
+__global__ void __launch_bounds__(kThreads, (MODE == kEncClassify ? 3 : 4))
+encode2_kernel(EncArgs a) {
+  constexpr int BPW = 32 / G;
+  constexpr int TB = kWarps * BPW;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  __shared__ uint32_t s_bytes[TB];
+  __shared__ unsigned s_w1[kWarps], s_w2[kWarps], s_w3[kWarps];
+  __shared__ long long s_tile;
+  __shared__ unsigned long long s_gbyte, s_gcnt;
+  __shared__ unsigned s_tile_bytes, s_tile_cps, s_tile_ext;
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int gi = lane / G, l = lane % G;
+  const bool tags = (MODE != kEncInts);
+  unsigned char *img = smem_dyn;
+  uint32_t *imgw = reinterpret_cast<uint32_t *>(img);
+
+  const long long n = (long long)a.n;
+  const int B = a.B;
+  const long long nblocks = (n + B - 1) / B;
+  const long long ntiles = (nblocks + TB - 1) / TB;
+
+  while (true) {
+    if (threadIdx.x == 0) s_tile = (long long)atomicAdd(a.tile_ctr, 1u);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= ntiles) break;
+
+    const int bi = warp * BPW + gi;
+    const long long blk = tile * TB + bi;
+    const long long base = blk * B;
+    const int len = (blk < nblocks) ? (int)((n - base) < B ? (n - base) : B) : 0;
+    const int e0 = 8 * l;
+    const int nv = len - e0 < 0 ? 0 : (len - e0 > 8 ? 8 : len - e0);
+    const long long i0 = base + e0;
+
+    // ---- phase 1: load, quantize, classify ----
+    float x[8];
+    int q[8];
+    unsigned types = 0;
+#pragma unroll
+    for (int t = 0; t < 8; t++) { x[t] = 0.f; q[t] = 0; }
+    if (MODE == kEncInts) {
+      if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.ints + i0) & 15) == 0)) {
+        const int4 u = __ldg(reinterpret_cast<const int4 *>(a.ints + i0));
+        const int4 w = __ldg(reinterpret_cast<const int4 *>(a.ints + i0) + 1);
+        q[0] = u.x; q[1] = u.y; q[2] = u.z; q[3] = u.w; q[4] = w.x; q[5] = w.y; q[6] = w.z; q[7] = w.w;
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; t++) if (t < nv) q[t] = __ldg(a.ints + i0 + t);
+      }
+    } else {
+      load_oct(a.data, i0, n, nv >= 8 ? 0xffu : ((1u << nv) - 1u), x);
+#pragma unroll
+      for (int t = 0; t < 8; t++) if (t < nv) q[t] = quantize(x[t], a.inv);
+      if (MODE == kEncClassify) {
+        if (nv > 0) types = classify_octet(a.data, n, i0, nv, x, a.g);
+      } else if (nv > 0) {
+        if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.types + i0) & 7) == 0)) {
+          const unsigned long long w = __ldg(reinterpret_cast<const unsigned long long *>(a.types + i0));
+#pragma unroll
+          for (int t = 0; t < 8; t++) types |= (unsigned)((w >> (8 * t)) & 3u) << (2 * t);
+        } else {
+#pragma unroll
+          for (int t = 0; t < 8; t++)
+            if (t < nv) types |= (unsigned)(a.types[i0 + t] & 3u) << (2 * t);
+        }
+      }
+    }
+    // deltas d = e0 + t use q[t + 1] - q[t]; q[8] is the next lane's q[0]
+    int qn = __shfl_down_sync(0xffffffffu, q[0], 1, G);
+    if (l == G - 1) qn = 0;  // blocks of at most 8G elements: no element 8G
+    const int cnt = len > 0 ? len - 1 : 0;
+    unsigned negm = 0, maxm = 0;
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      if (e0 + t < cnt) {
+        const int nx = (t < 7) ? q[t + 1] : qn;
+        const unsigned ud = (unsigned)nx - (unsigned)q[t];
+        const bool ng = (int)ud < 0;
+        const unsigned m = ng ? 0u - ud : ud;
+        if (ng) negm |= 1u << t;
+        maxm = m > maxm ? m : maxm;
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      const unsigned u = __shfl_xor_sync(0xffffffffu, maxm, o);
+      maxm = u > maxm ? u : maxm;
+    }
+    const unsigned bc = bitcount(maxm);
+    if (l == 0) s_bytes[bi] = len ? block_bytes((unsigned)len, bc, tags) : 0u;
+    unsigned cpm = 0, exm = 0;
+    if (MODE == kEncClassify) {
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        const unsigned ty = (types >> (2 * t)) & 3u;
+        if (ty) cpm |= 1u << t;
+        if (ty == 1u || ty == 2u) exm |= 1u << t;
+      }
+    }
+    __syncthreads();
+
+    // ---- phase 2: tile scans (block bytes; per-thread CP / extremum counts) ----
+    unsigned tbytes, tcps, text;
+    const unsigned bv = (threadIdx.x < TB) ? s_bytes[threadIdx.x] : 0u;
+    const unsigned boff = cta_excl_scan(bv, s_w1, &tbytes);
+    const unsigned cpo = cta_excl_scan((unsigned)__popc(cpm), s_w2, &tcps);
+    const unsigned exo = cta_excl_scan((unsigned)__popc(exm), s_w3, &text);
+    __syncthreads();
+    if (threadIdx.x < TB) s_bytes[threadIdx.x] = boff;
+    if (threadIdx.x == 0) {
+      s_tile_bytes = tbytes;
+      s_tile_cps = tcps;
+      s_tile_ext = text;
+      publish_aggregate(a.desc, tile, tbytes, ((unsigned long long)tcps << 32) | text);
+    }
+    __syncthreads();
+    const unsigned tile_bytes = s_tile_bytes;
+
+    // ---- phase 3: pack the octet into the tile image ----
+    if (a.out != nullptr && nv > 0) {
+      unsigned p = s_bytes[bi];
+      if (l == 0) {
+        const unsigned an = (unsigned)q[0];
+        img[p] = (unsigned char)an;
+        img[p + 1] = (unsigned char)(an >> 8);
+        img[p + 2] = (unsigned char)(an >> 16);
+        img[p + 3] = (unsigned char)(an >> 24);
+        if (len > 1) img[p + 4] = (unsigned char)bc;
+      }
+      p += 4;
+      if (len > 1) {
+        p += 1;
+        if (bc) {
+          unsigned mags[8];
+#pragma unroll
+          for (int t = 0; t < 8; t++) {
+            mags[t] = 0;
+            if (e0 + t < cnt) {
+              const int nx = (t < 7) ? q[t + 1] : qn;
+              const unsigned ud = (unsigned)nx - (unsigned)q[t];
+              mags[t] = ((int)ud < 0) ? 0u - ud : ud;
+            }
+          }
+          const unsigned sbytes = (unsigned)(cnt + 7) / 8u;
+          const bool has_d = e0 < cnt;
+          if (has_d) {
+            // sign byte: delta e0 + t at bit 7 - t
+            img[p + l] = (unsigned char)(__brev(negm) >> 24);
+          }
+          p += sbytes;
+          const unsigned fb = bc >> 3, rem = bc & 7u;
+          if (fb) {
+            if (has_d) {
+#pragma unroll
+              for (int t = 0; t < 8; t++) {
+                if (e0 + t < cnt) {
+                  unsigned v = mags[t] >> rem;
+                  const unsigned o = (unsigned)(e0 + t) * fb;
+                  for (unsigned u = 0; u < fb; u++) { img[p + o + u] = (unsigned char)v; v >>= 8; }
+                }
+              }
+            }
+            p += fb * (unsigned)cnt;
+          }
+          if (rem) {
+            const unsigned rbytes = (rem * (unsigned)cnt - 1u) / 8u + 1u;
+            if (has_d) {
+              const unsigned mask = (1u << rem) - 1u;
+              unsigned long long acc = 0;
+#pragma unroll
+              for (int t = 0; t < 8; t++) acc = (acc << rem) | (unsigned long long)(mags[t] & mask);
+              // the octet's 8*rem bits are exactly rem bytes at byte l*rem
+              const unsigned ob = (unsigned)l * rem;
+              for (unsigned u = 0; u < rem; u++)
+                if (ob + u < rbytes) img[p + ob + u] = (unsigned char)(acc >> (8 * (rem - 1u - u)));
+            }
+            p += rbytes;
+          }
+        }
+      }
+      if (tags) {
+        const unsigned tb = ((unsigned)len + 3u) / 4u;
+        // tag byte for elements 4j..4j+3: element 4j in the top two bits
+        const unsigned t0 = ((types & 3u) << 6) | (((types >> 2) & 3u) << 4) | (((types >> 4) & 3u) << 2) |
+                            ((types >> 6) & 3u);
+        const unsigned t1 = (((types >> 8) & 3u) << 6) | (((types >> 10) & 3u) << 4) |
+                            (((types >> 12) & 3u) << 2) | ((types >> 14) & 3u);
+        if (2u * l < tb) img[p + 2 * l] = (unsigned char)t0;
+        if (2u * l + 1u < tb) img[p + 2 * l + 1] = (unsigned char)t1;
+      }
+    }
+
+    // ---- phase 4: look-back (whole CTA) ----
+    {
+      const Prefix pf = lookback_cta(a.desc, tile, tile_bytes,
+                                     ((unsigned long long)s_tile_cps << 32) | s_tile_ext, a.err);
+      if (threadIdx.x == 0) {
+        s_gbyte = pf.bytes;
+        s_gcnt = pf.cnt;
+        if (tile == ntiles - 1 && a.total) {
+          a.total[0] = pf.bytes + tile_bytes;
+          a.total[1] = (pf.cnt >> 32) + s_tile_cps;
+          a.total[2] = (pf.cnt & 0xffffffffull) + s_tile_ext;
+        }
+      }
+    }
+    __syncthreads();
+    const unsigned long long G0 = s_gbyte;
+    const bool fits = a.out != nullptr && (G0 + tile_bytes) <= a.out_cap;
+    if (a.out != nullptr && !fits && threadIdx.x == 0) atomicExch(a.err, kErrOutputOverflow);
+    if (a.blk_off && threadIdx.x < TB) {
+      const long long b2 = tile * TB + threadIdx.x;
+      if (b2 < nblocks) a.blk_off[b2] = G0 + s_bytes[threadIdx.x];
+    }
+
+    // ---- phase 5: write the tile image (aligned 16-byte stores in the middle) ----
+    if (fits && tile_bytes) {
+      unsigned char *dst = a.out + G0;
+      unsigned head = (unsigned)((16u - (unsigned)(reinterpret_cast<uintptr_t>(dst) & 15u)) & 15u);
+      if (head > tile_bytes) head = tile_bytes;
+      if (threadIdx.x < head) dst[threadIdx.x] = img[threadIdx.x];
+      const unsigned nq = (tile_bytes - head) >> 4;
+      const unsigned sh = 8u * (head & 3u);
+      const unsigned w0 = head >> 2;
+      uint4 *dq = reinterpret_cast<uint4 *>(dst + head);
+      for (unsigned qd = threadIdx.x; qd < nq; qd += kThreads) {
+        const unsigned wi = w0 + 4u * qd;
+        uint4 v;
+        if (sh) {
+          v.x = __funnelshift_r(imgw[wi], imgw[wi + 1], sh);
+          v.y = __funnelshift_r(imgw[wi + 1], imgw[wi + 2], sh);
+          v.z = __funnelshift_r(imgw[wi + 2], imgw[wi + 3], sh);
+          v.w = __funnelshift_r(imgw[wi + 3], imgw[wi + 4], sh);
+        } else {
+          v.x = imgw[wi]; v.y = imgw[wi + 1]; v.z = imgw[wi + 2]; v.w = imgw[wi + 3];
+        }
+        dq[qd] = v;
+      }
+      const unsigned t0b = head + 16u * nq;
+      if (t0b + threadIdx.x < tile_bytes) dst[t0b + threadIdx.x] = img[t0b + threadIdx.x];
+    }
+
+    // ---- phase 6: critical points in raster order (thread order == raster order) ----
+    if (MODE == kEncClassify && a.cp_mode != kCpNone && cpm) {
+      unsigned long long ci = (s_gcnt >> 32) + cpo;
+      unsigned long long ei = (s_gcnt & 0xffffffffull) + exo;
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        if (!(cpm & (1u << t))) continue;
+        const unsigned ty = (types >> (2 * t)) & 3u;
+        const bool ext = (ty == 1u || ty == 2u);
+        const long long idx = i0 + t;
+        if (ci < a.cp_cap) {
+          const float xv = __ldg(a.data + idx);
+          if (a.cp_mode == kCpPairs) {
+            reinterpret_cast<uint2 *>(a.cp_out)[ci] = make_uint2(float_code(xv), ext ? (uint32_t)ei : kNoExtremum);
+          } else {
+            long long r;
+            const int bin = quant_bin(xv, a.eb, a.inv);
+            if (a.g.nd == 2) {
+              const long long row = fdivmod(idx, a.g.d3, a.g.m_d3, r);
+              int *rec = reinterpret_cast<int *>(a.cp_out) + 5 * ci;
+              rec[0] = (int)row; rec[1] = (int)r; rec[2] = (int)ty; rec[3] = bin; rec[4] = 0;
+            } else {
+              long long z;
+              const long long x3 = fdivmod(idx, a.g.plane, a.g.m_plane, r);
+              const long long y3 = fdivmod(r, a.g.d3, a.g.m_d3, z);
+              int *rec = reinterpret_cast<int *>(a.cp_out) + 6 * ci;
+              rec[0] = (int)x3; rec[1] = (int)y3; rec[2] = (int)z; rec[3] = (int)ty; rec[4] = bin; rec[5] = 0;
+            }
+          }
+        }
+        ci++;
+        if (ext) ei++;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// reads 8 bytes starting at an arbitrary shared-memory byte position
+__device__ __forceinline__ unsigned long long ld_bytes8(const unsigned char *img, unsigned p) {
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(img);
+  const unsigned wi = p >> 2, sh = 8u * (p & 3u);
+  const uint32_t a = w[wi], b = w[wi + 1], c = w[wi + 2];
+  const uint32_t lo = sh ? __funnelshift_r(a, b, sh) : a;
+  const uint32_t hi = sh ? __funnelshift_r(b, c, sh) : b;
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+template <bool TAGS, int G>
+__global__ void __launch_bounds__(kThreads)
+decode2_kernel(DecArgs a) {
+  constexpr int BPW = 32 / G;
+  constexpr int TB = kWarps * BPW;
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  __shared__ unsigned long long s_off[TB + 1];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int gi = lane / G, l = lane % G;
+  unsigned char *img = smem_dyn;
+
+  const long long n = (long long)a.n;
+  const int B = a.B;
+  const long long nblocks = (n + B - 1) / B;
+  const long long b0 = (long long)blockIdx.x * TB;
+  if (b0 >= nblocks) return;
+  const int nb = (int)((nblocks - b0) < TB ? (nblocks - b0) : TB);
+  for (int t = threadIdx.x; t <= nb; t += kThreads) {
+    unsigned long long o;
+    if (t < nb) o = a.blk_off[b0 + t];
+    else o = (b0 + nb < nblocks) ? a.blk_off[b0 + nb] : a.payload_len;
+    s_off[t] = o;
+  }
+  __syncthreads();
+  const unsigned long long lo = s_off[0] & ~3ull;
+  unsigned long long hi = s_off[nb];
+  if (hi > a.payload_len) hi = a.payload_len;
+  if (s_off[0] > hi || hi - lo > a.img_cap) {
+    if (threadIdx.x == 0) atomicExch(a.err, kErrMalformed);
+    return;
+  }
+  {
+    const unsigned long long span = hi - lo;
+    const unsigned long long full_words = (a.payload_len & ~3ull);
+    const uint32_t nw = (uint32_t)((span + 3) >> 2);
+    const uint32_t *srcw = reinterpret_cast<const uint32_t *>(a.payload + lo);
+    uint32_t *imgw = reinterpret_cast<uint32_t *>(img);
+    for (uint32_t w = threadIdx.x; w < nw; w += kThreads) {
+      const unsigned long long gpos = lo + 4ull * w;
+      uint32_t v;
+      if (gpos + 4 <= full_words) {
+        v = __ldg(srcw + w);
+      } else {
+        v = 0;
+        for (int t = 0; t < 4; t++)
+          if (gpos + t < a.payload_len) v |= (uint32_t)a.payload[gpos + t] << (8 * t);
+      }
+      imgw[w] = v;
+    }
+    if (threadIdx.x < 4) imgw[nw + threadIdx.x] = 0;  // padding for 8-byte window reads
+  }
+  __syncthreads();
+
+  const int bi = warp * BPW + gi;
+  const bool have = bi < nb;
+  const long long blk = b0 + bi;
+  const long long base = blk * B;
+  const int len = have ? (int)((n - base) < B ? (n - base) : B) : 0;
+  const int e0 = 8 * l;
+  const int nv = len - e0 < 0 ? 0 : (len - e0 > 8 ? 8 : len - e0);
+  bool ok = have;
+  unsigned start = 0, bend = 0;
+  if (ok) {
+    if (s_off[bi] < s_off[0] || s_off[bi] + 4 > hi || s_off[bi + 1] < s_off[bi] || s_off[bi + 1] > s_off[nb])
+      ok = false;
+    start = (unsigned)(s_off[bi] - lo);
+    bend = (unsigned)((s_off[bi + 1] < hi ? s_off[bi + 1] : hi) - lo);
+  }
+  unsigned bc = 0;
+  int anchor = 0;
+  const int cnt = len > 0 ? len - 1 : 0;
+  if (ok) {
+    anchor = (int)((unsigned)img[start] | ((unsigned)img[start + 1] << 8) | ((unsigned)img[start + 2] << 16) |
+                   ((unsigned)img[start + 3] << 24));
+    if (len > 1) bc = (start + 4 < bend) ? img[start + 4] : 0u;
+    if (bc > 32u || start + block_bytes((unsigned)len, bc, TAGS) > bend) ok = false;
+  }
+  if (have && !ok && l == 0) atomicExch(a.err, kErrMalformed);
+  // deltas e0 .. e0+7
+  unsigned dl[8];
+  unsigned tsum = 0;
+#pragma unroll
+  for (int t = 0; t < 8; t++) dl[t] = 0;
+  unsigned p = start + 4 + (len > 1 ? 1u : 0u);
+  if (ok && bc && e0 < cnt) {
+    const unsigned sbytes = (unsigned)(cnt + 7) / 8u;
+    const unsigned negb = img[p + l];
+    const unsigned mag = p + sbytes;
+    const unsigned fb = bc >> 3, rem = bc & 7u;
+    unsigned long long rbits = 0;
+    if (rem) {
+      const unsigned rsec = mag + fb * (unsigned)cnt;
+      // this octet's remainder fields: rem bytes at byte l*rem, MSB first
+      const unsigned long long w = ld_bytes8(img, rsec + (unsigned)l * rem);
+      // bytes in stream order -> big-endian integer of rem bytes
+      unsigned long long be = 0;
+#pragma unroll
+      for (int u = 0; u < 7; u++)
+        if ((unsigned)u < rem) be = (be << 8) | ((w >> (8 * u)) & 0xffull);
+      rbits = be;
+    }
+    unsigned long long fw = 0;
+    if (fb == 1) fw = ld_bytes8(img, mag + (unsigned)e0);
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      if (e0 + t < cnt) {
+        unsigned v = 0;
+        if (rem) v = (unsigned)(rbits >> (rem * (7u - t))) & ((1u << rem) - 1u);
+        if (fb == 1) {
+          v |= (unsigned)((fw >> (8 * t)) & 0xffull) << rem;
+        } else if (fb) {
+          unsigned full = 0;
+          const unsigned o = mag + (unsigned)(e0 + t) * fb;
+          for (unsigned u = 0; u < fb; u++) full |= (unsigned)img[o + u] << (8 * u);
+          v |= full << rem;
+        }
+        dl[t] = ((negb >> (7 - t)) & 1u) ? (0u - v) : v;
+        tsum += dl[t];
+      }
+    }
+  }
+  // exclusive scan of the octet sums inside the group
+  unsigned inc = tsum;
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) {
+    const unsigned u = __shfl_up_sync(0xffffffffu, inc, o, G);
+    if (l >= o) inc += u;
+  }
+  unsigned v = (unsigned)anchor + inc - tsum;
+  unsigned n_ext = 0;
+  if (ok && nv > 0) {
+    int qv[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++) { qv[t] = (int)v; v += dl[t]; }
+    const long long i0 = base + e0;
+    if (a.out_f) {
+      float f[8];
+#pragma unroll
+      for (int t = 0; t < 8; t++) f[t] = __fmul_rn((float)qv[t], a.eb);
+      if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.out_f + i0) & 15) == 0)) {
+        reinterpret_cast<float4 *>(a.out_f + i0)[0] = make_float4(f[0], f[1], f[2], f[3]);
+        reinterpret_cast<float4 *>(a.out_f + i0)[1] = make_float4(f[4], f[5], f[6], f[7]);
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; t++) if (t < nv) a.out_f[i0 + t] = f[t];
+      }
+    }
+    if (a.out_i) {
+      if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.out_i + i0) & 15) == 0)) {
+        reinterpret_cast<int4 *>(a.out_i + i0)[0] = make_int4(qv[0], qv[1], qv[2], qv[3]);
+        reinterpret_cast<int4 *>(a.out_i + i0)[1] = make_int4(qv[4], qv[5], qv[6], qv[7]);
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; t++) if (t < nv) a.out_i[i0 + t] = qv[t];
+      }
+    }
+    if (TAGS) {
+      const unsigned tsec = start + block_bytes((unsigned)len, bc, true) - ((unsigned)len + 3u) / 4u;
+      const unsigned tb = ((unsigned)len + 3u) / 4u;
+      const unsigned b0t = (2u * l < tb) ? img[tsec + 2 * l] : 0u;
+      const unsigned b1t = (2u * l + 1u < tb) ? img[tsec + 2 * l + 1] : 0u;
+      unsigned ty[8];
+      ty[0] = (b0t >> 6) & 3u; ty[1] = (b0t >> 4) & 3u; ty[2] = (b0t >> 2) & 3u; ty[3] = b0t & 3u;
+      ty[4] = (b1t >> 6) & 3u; ty[5] = (b1t >> 4) & 3u; ty[6] = (b1t >> 2) & 3u; ty[7] = b1t & 3u;
+      unsigned ne = 0;
+#pragma unroll
+      for (int t = 0; t < 8; t++) if (t < nv && (ty[t] == 1u || ty[t] == 2u)) ne++;
+      if (a.fn_u8) {
+        if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.fn_u8 + i0) & 7) == 0)) {
+          unsigned long long w = 0;
+#pragma unroll
+          for (int t = 0; t < 8; t++) w |= (unsigned long long)ty[t] << (8 * t);
+          *reinterpret_cast<unsigned long long *>(a.fn_u8 + i0) = w;
+        } else {
+#pragma unroll
+          for (int t = 0; t < 8; t++) if (t < nv) a.fn_u8[i0 + t] = (unsigned char)ty[t];
+        }
+      }
+      if (a.fn_i) {
+#pragma unroll
+        for (int t = 0; t < 8; t++) if (t < nv) a.fn_i[i0 + t] = (int)ty[t];
+      }
+      n_ext = ne;
+    }
+  }
+  if (TAGS && a.ext_count) {
+    n_ext = __reduce_add_sync(0xffffffffu, n_ext);
+    if (lane == 0 && n_ext) atomicAdd(a.ext_count, (unsigned long long)n_ext);
+  }
+}
+
+}  // namespace tsz

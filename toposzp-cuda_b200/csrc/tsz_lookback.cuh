@@ -100,3 +100,67 @@ __device__ inline Prefix lookback(TileDesc *desc, long long t, unsigned long lon
 }
 
 }  // namespace tsz
+
+namespace tsz {
+
+// CTA-wide look-back: all kThreads threads of the CTA call it after the
+// tile's aggregate has been published.  Each round inspects kThreads
+// predecessors at once, so a walk back over P in-flight tiles takes about
+// P / kThreads rounds instead of P / 32.
+__device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long long agg_bytes,
+                                      unsigned long long agg_cnt, int *err) {
+  __shared__ unsigned s_first[kWarps];
+  __shared__ unsigned long long s_b[kWarps], s_c[kWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  Prefix ex{0ull, 0ull};
+  if (t == 0) return ex;
+  long long base = t - 1;
+  bool timed_out = false;
+  while (true) {
+    const long long idx = base - (long long)threadIdx.x;
+    unsigned long long st = (2ull << kStatShift);
+    if (idx >= 0) {
+      st = ld_acquire_u64(&desc[idx].status);
+      int spins = 0;
+      while ((st >> kStatShift) == 0ull) {
+        if (++spins > kSpinLimit) { timed_out = true; break; }
+        __nanosleep(spins < 64 ? 32 : 256);
+        st = ld_acquire_u64(&desc[idx].status);
+      }
+    }
+    unsigned long long flag = st >> kStatShift;
+    if (flag == 0ull) flag = 2ull;
+    // nearest predecessor (smallest thread index) holding an inclusive prefix
+    const unsigned wm = __ballot_sync(0xffffffffu, flag == 2ull);
+    if (lane == 0) s_first[warp] = wm ? (unsigned)(warp * 32 + __ffs(wm) - 1) : 0xffffffffu;
+    __syncthreads();
+    unsigned first = 0xffffffffu;
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) first = min(first, s_first[w]);
+    unsigned long long b = 0, c = 0;
+    if ((unsigned)threadIdx.x <= first && idx >= 0 && (st >> kStatShift) != 0ull) {
+      b = st & kByteMask;
+      c = (flag == 2ull) ? ld_relaxed_u64(&desc[idx].inc_cnt) : ld_relaxed_u64(&desc[idx].agg_cnt);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) { s_b[warp] = b; s_c[warp] = c; }
+    __syncthreads();
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) { ex.bytes += s_b[w]; ex.cnt += s_c[w]; }
+    __syncthreads();
+    if (first != 0xffffffffu) break;
+    base -= kThreads;
+  }
+  if (timed_out) atomicExch(err, kErrLookbackTimeout);
+  if (threadIdx.x == 0) {
+    st_relaxed_u64(&desc[t].inc_cnt, ex.cnt + agg_cnt);
+    st_release_u64(&desc[t].status, (2ull << kStatShift) | ((ex.bytes + agg_bytes) & kByteMask));
+  }
+  return ex;
+}
+
+}  // namespace tsz

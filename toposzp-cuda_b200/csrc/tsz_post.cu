@@ -4,17 +4,19 @@
 //
 // Each reference pass visits points in raster order and updates them in
 // place, so a point sees the FINAL values of earlier points and the
-// PRE-PASS values of later points.  Here one kernel per pass reproduces that:
+// PRE-PASS values of later points.  Only a pass's candidates change (extrema
+// for the stencil and enforcement passes, lost saddles for RBF, saddles for
+// the axis-pattern stencil), so the passes run over compact candidate lists:
 //   * F holds the field before the pass and is not written during the pass;
 //   * a candidate's result goes to S[e] = (generation << 32) | float bits;
-//   * reading neighbour q: if q is an earlier candidate of this pass, wait for
-//     S[q] to carry this pass's generation and use it; otherwise read F[q];
-//   * tiles of 2048 points are claimed in raster order through an atomic
-//     counter, so every awaited point belongs to a CTA that is already
-//     running, and waits are bounded (kErrWaitTimeout).
-// A scatter kernel then copies the pass results into F.  Floating-point
-// expressions use explicit round-to-nearest intrinsics so that no multiply-add
-// is contracted (the reference host code is compiled without contraction).
+//   * a candidate is computed once every EARLIER candidate it reads has its
+//     result for this pass (a neighbour read then returns that result; every
+//     other read returns F); otherwise it is deferred to the next round.
+// Rounds repeat over the deferred items until none is left (their number is
+// the longest chain of adjacent candidates in raster order), and a list
+// scatter then copies the pass results into F.  Floating-point expressions use
+// explicit round-to-nearest intrinsics so that no multiply-add is contracted
+// (the reference host code is compiled without contraction).
 #include <cfloat>
 
 #include "tsz_lookback.cuh"
@@ -26,6 +28,28 @@
 namespace tsz {
 
 enum { kPassStencil = 0, kPassEnforce = 1, kPassRbf = 2, kPassAxis = 3 };
+
+// CTA-wide exclusive scan of one value per thread (kPostThreads threads)
+__device__ __forceinline__ unsigned cta_excl_scan_post(unsigned v, unsigned *s_warp, unsigned *total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  unsigned wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < 256 / 32; w++) {
+    const unsigned sw = s_warp[w];
+    if (w < warp) wpre += sw;
+    tot += sw;
+  }
+  *total = tot;
+  return wpre + inc - v;
+}
 constexpr int kPostThreads = 256;
 constexpr int kPostPer = 8;
 constexpr int kPostTile = kPostThreads * kPostPer;
@@ -46,6 +70,8 @@ struct PostArgs {
   float eps;
   unsigned gen;
   unsigned long long *S;
+  const unsigned *L;            // lock bitmap: interior point next to an interior extremum
+  const unsigned *R;            // RBF candidates (lost saddles) bitmap
   TileDesc *desc;
   unsigned *tile_ctr;
   int *err;
@@ -79,20 +105,7 @@ __device__ __forceinline__ bool interior(const Geom &g, const C3 &c) {
 }
 __device__ __forceinline__ bool interior_at(const Geom &g, long long q) { return interior(g, coords(g, q)); }
 
-__device__ __forceinline__ float wait_result(const PostArgs &a, long long q) {
-  unsigned long long v = ld_rlx(&a.S[q]);
-  int spins = 0;
-  while ((unsigned)(v >> 32) != a.gen) {
-    if (++spins > kSpinLimit) { atomicExch(a.err, kErrWaitTimeout); return a.F[q]; }
-    __nanosleep(spins < 32 ? 20 : 200);
-    v = ld_rlx(&a.S[q]);
-  }
-  return __uint_as_float((unsigned)v);
-}
-
-// ----------------------------------------------------------------------------
-// candidate predicates (evaluated on F, which is stable during a pass)
-// ----------------------------------------------------------------------------
+// 4/6-neighbour classification on F (stable during a pass)
 __device__ __forceinline__ int classify_F(const PostArgs &a, long long q) {
   const float *F = a.F;
   if (a.g.nd == 2)
@@ -101,26 +114,72 @@ __device__ __forceinline__ int classify_F(const PostArgs &a, long long q) {
                    F[q + 1]);
 }
 
+__device__ __forceinline__ bool bit_at(const unsigned *b, long long q) { return (b[q >> 5] >> (q & 31)) & 1u; }
+
+// q is a candidate of pass PASS (q_interior: q lies in the interior)
 template <int PASS>
-__device__ __forceinline__ bool is_cand(const PostArgs &a, long long q) {
+__device__ __forceinline__ bool is_cand_known(const PostArgs &a, long long q, bool q_interior) {
+  if (!q_interior) return false;
+  if (PASS == kPassRbf) return bit_at(a.R, q);
   const int t = ty(a, q);
-  if (PASS == kPassStencil || PASS == kPassEnforce) {
-    if (t != 1 && t != 2) return false;
-    return interior_at(a.g, q);
-  }
-  if (t != 3) return false;
-  if (!interior_at(a.g, q)) return false;
-  // the axis-pattern pass re-tests every saddle against the current values
-  // inside the update itself (example/test_cuda_topology_3d.cu:203-206)
-  if (PASS == kPassAxis) return true;
-  return classify_F(a, q) != 3;
+  if (PASS == kPassStencil || PASS == kPassEnforce) return t == 1 || t == 2;
+  return t == 3;
 }
 
-// value of neighbour q as the serial pass would see it from point e (q != e)
+__device__ __forceinline__ bool interior_off(const PostArgs &a, const C3 &c, int dx, int dy, int dz) {
+  bool qi = c.y + dy >= 1 && c.y + dy <= a.g.d2 - 2 && c.z + dz >= 1 && c.z + dz <= a.g.d3 - 2;
+  if (a.g.nd == 3) qi = qi && c.x + dx >= 1 && c.x + dx <= a.g.d1 - 2;
+  return qi;
+}
+
+// result of candidate q for the current pass, or -1 when not available yet
+__device__ __forceinline__ bool result_ready(const PostArgs &a, long long q) {
+  return (unsigned)(ld_rlx(&a.S[q]) >> 32) == a.gen;
+}
+
+// neighbour of e at offset (dx, dy, dz) (dx = 0 in 2D) as the serial pass
+// sees it; earlier candidates are resolved before e is computed
 template <int PASS>
-__device__ __forceinline__ float val(const PostArgs &a, long long e, long long q) {
-  if (q < e && is_cand<PASS>(a, q)) return wait_result(a, q);
+__device__ __forceinline__ float valo(const PostArgs &a, long long e, const C3 &c, int dx, int dy, int dz) {
+  const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
+  if (q > e) return a.F[q];
+  if (is_cand_known<PASS>(a, q, interior_off(a, c, dx, dy, dz)))
+    return __uint_as_float((unsigned)ld_rlx(&a.S[q]));
   return a.F[q];
+}
+
+// every earlier candidate that e may read has its result for this pass
+template <int PASS, int ND>
+__device__ bool deps_ready(const PostArgs &a, long long e, const C3 &c) {
+  if (PASS == kPassStencil || PASS == kPassEnforce) {
+    const int nd3 = (ND == 3) ? 1 : 0;
+    const int offs[3][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}};
+    for (int k = 1 - nd3; k < 3; k++) {
+      const int dx = offs[k][0], dy = offs[k][1], dz = offs[k][2];
+      const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
+      if (is_cand_known<PASS>(a, q, interior_off(a, c, dx, dy, dz)) && !result_ready(a, q)) return false;
+    }
+    return true;
+  }
+  // RBF / axis pattern: earlier points of the 3x3(x3) box and the points two
+  // steps back along each axis
+  const int xr = (ND == 3) ? 1 : 0;
+  for (int dx = -xr; dx <= 0; dx++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dz = -1; dz <= 1; dz++) {
+        if (dx == 0 && (dy > 0 || (dy == 0 && dz >= 0))) continue;
+        const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
+        if (is_cand_known<PASS>(a, q, interior_off(a, c, dx, dy, dz)) && !result_ready(a, q)) return false;
+      }
+  const int far[3][3] = {{-2, 0, 0}, {0, -2, 0}, {0, 0, -2}};
+  for (int k = (ND == 3 ? 0 : 1); k < 3; k++) {
+    const int dx = far[k][0], dy = far[k][1], dz = far[k][2];
+    if (ND == 3 && c.x + dx < 0) continue;
+    if (c.y + dy < 0 || c.z + dz < 0) continue;
+    const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
+    if (is_cand_known<PASS>(a, q, interior_off(a, c, dx, dy, dz)) && !result_ready(a, q)) return false;
+  }
+  return true;
 }
 
 // ----------------------------------------------------------------------------
@@ -133,15 +192,14 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) {
 }
 
 // 2D stencil (example/test_cuda_topology.cu:118-165)
-__device__ float stencil2(const PostArgs &a, long long e, int t, int s) {
-  const long long cols = a.g.d3;
+__device__ float stencil2(const PostArgs &a, long long e, const C3 &c, int t, int s) {
   const float o = a.O[e];
   const float hi = __fadd_rn(o, a.eb), lo = __fsub_rn(o, a.eb);
   float m = a.F[e];
-  const long long nb[4] = {e - cols, e + cols, e - 1, e + 1};
+  const int ofs[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    const float v = val<kPassStencil>(a, e, nb[k]);
+    const float v = valo<kPassStencil>(a, e, c, 0, ofs[k][0], ofs[k][1]);
     if (t == 1 ? (v > m) : (v < m)) m = v;
   }
   float target;
@@ -152,14 +210,14 @@ __device__ float stencil2(const PostArgs &a, long long e, int t, int s) {
 }
 
 // 3D stencil (example/test_cuda_topology_3d.cu:77-128)
-__device__ float stencil3(const PostArgs &a, long long e, int t, int s) {
+__device__ float stencil3(const PostArgs &a, long long e, const C3 &c, int t, int s) {
   const float o = a.O[e];
   const float d = __fmul_rn(a.eb, 0.999f);
   const float hi = __fadd_rn(o, d), lo = __fsub_rn(o, d);
   const long long pl = a.g.plane, d3 = a.g.d3;
-  const float xm = val<kPassStencil>(a, e, e - pl), xp = a.F[e + pl];
-  const float ym = val<kPassStencil>(a, e, e - d3), yp = a.F[e + d3];
-  const float zm = val<kPassStencil>(a, e, e - 1), zp = a.F[e + 1];
+  const float xm = valo<kPassStencil>(a, e, c, -1, 0, 0), xp = a.F[e + pl];
+  const float ym = valo<kPassStencil>(a, e, c, 0, -1, 0), yp = a.F[e + d3];
+  const float zm = valo<kPassStencil>(a, e, c, 0, 0, -1), zp = a.F[e + 1];
   // later neighbours read through val too (candidates later than e use F)
   float target;
   if (t == 1) {
@@ -175,7 +233,7 @@ __device__ float stencil3(const PostArgs &a, long long e, int t, int s) {
 
 // enforcement (example/test_cuda_topology.cu:168-198, _3d.cu:131-167)
 template <int ND>
-__device__ float enforce(const PostArgs &a, long long e, int t) {
+__device__ float enforce(const PostArgs &a, long long e, const C3 &c, int t) {
   const float o = a.O[e];
   const float d = __fmul_rn(a.eb, 0.999f);
   const float hi = __fadd_rn(o, d), lo = __fsub_rn(o, d);
@@ -184,14 +242,14 @@ __device__ float enforce(const PostArgs &a, long long e, int t) {
   float m;
   if (ND == 2) {
     const long long cols = a.g.d3;
-    const float n = val<kPassEnforce>(a, e, e - cols), s = a.F[e + cols];
-    const float w = val<kPassEnforce>(a, e, e - 1), ea = a.F[e + 1];
+    const float n = valo<kPassEnforce>(a, e, c, 0, -1, 0), s = a.F[e + cols];
+    const float w = valo<kPassEnforce>(a, e, c, 0, 0, -1), ea = a.F[e + 1];
     m = (t == 1) ? fmaxf(fmaxf(n, s), fmaxf(w, ea)) : fminf(fminf(n, s), fminf(w, ea));
   } else {
     const long long pl = a.g.plane, d3 = a.g.d3;
-    const float xm = val<kPassEnforce>(a, e, e - pl), xp = a.F[e + pl];
-    const float ym = val<kPassEnforce>(a, e, e - d3), yp = a.F[e + d3];
-    const float zm = val<kPassEnforce>(a, e, e - 1), zp = a.F[e + 1];
+    const float xm = valo<kPassEnforce>(a, e, c, -1, 0, 0), xp = a.F[e + pl];
+    const float ym = valo<kPassEnforce>(a, e, c, 0, -1, 0), yp = a.F[e + d3];
+    const float zm = valo<kPassEnforce>(a, e, c, 0, 0, -1), zp = a.F[e + 1];
     m = (t == 1) ? fmaxf(fmaxf(xm, xp), fmaxf(fmaxf(ym, yp), fmaxf(zm, zp)))
                  : fminf(fminf(xm, xp), fminf(fminf(ym, yp), fminf(zm, zp)));
   }
@@ -207,34 +265,7 @@ __device__ float enforce(const PostArgs &a, long long e, int t) {
   return (cur > tg) ? tg : cur;
 }
 
-// lock: point q (interior) has an interior extremum within Chebyshev distance 1
-__device__ bool locked2(const PostArgs &a, long long q) {
-  const C3 c = coords(a.g, q);
-  if (c.y < 1 || c.y > a.g.d2 - 2 || c.z < 1 || c.z > a.g.d3 - 2) return false;
-  for (int da = -1; da <= 1; da++)
-    for (int db = -1; db <= 1; db++) {
-      const long long ii = c.y + da, jj = c.z + db;
-      if (ii < 1 || ii > a.g.d2 - 2 || jj < 1 || jj > a.g.d3 - 2) continue;
-      const int t = ty(a, ii * a.g.d3 + jj);
-      if (t == 1 || t == 2) return true;
-    }
-  return false;
-}
-
-__device__ bool locked3(const PostArgs &a, long long q) {
-  const C3 c = coords(a.g, q);
-  if (!interior(a.g, c)) return false;
-  for (int da = -1; da <= 1; da++)
-    for (int db = -1; db <= 1; db++)
-      for (int dc = -1; dc <= 1; dc++) {
-        const long long xx = c.x + da, yy = c.y + db, zz = c.z + dc;
-        if (xx < 1 || xx > a.g.d1 - 2 || yy < 1 || yy > a.g.d2 - 2 || zz < 1 || zz > a.g.d3 - 2)
-          continue;
-        const int t = ty(a, xx * a.g.plane + yy * a.g.d3 + zz);
-        if (t == 1 || t == 2) return true;
-      }
-  return false;
-}
+__device__ __forceinline__ bool locked(const PostArgs &a, long long q) { return bit_at(a.L, q); }
 
 __device__ __forceinline__ int cls4_eps(float c, float n, float s, float w, float e, float eps) {
   const float np = __fadd_rn(n, eps), sp = __fadd_rn(s, eps), wp = __fadd_rn(w, eps), ep = __fadd_rn(e, eps);
@@ -255,12 +286,12 @@ __device__ float rbf2(const PostArgs &a, long long e, const C3 &c, bool &ok) {
   float v[3][3];
   for (int da = -1; da <= 1; da++)
     for (int db = -1; db <= 1; db++)
-      v[da + 1][db + 1] = (da == 0 && db == 0) ? a.F[e] : val<kPassRbf>(a, e, e + da * cols + db);
+      v[da + 1][db + 1] = (da == 0 && db == 0) ? a.F[e] : valo<kPassRbf>(a, e, c, 0, da, db);
   double num = 0.0, den = 0.0;
   for (int da = -1; da <= 1; da++)
     for (int db = -1; db <= 1; db++) {
       double ww = c_w2[(da + 1) * 3 + (db + 1)];
-      if (locked2(a, e + da * cols + db)) ww = __dmul_rn(ww, 0.4);
+      if (locked(a, e + da * cols + db)) ww = __dmul_rn(ww, 0.4);
       num = __dadd_rn(num, __dmul_rn(ww, (double)v[da + 1][db + 1]));
       den = __dadd_rn(den, ww);
     }
@@ -290,10 +321,10 @@ __device__ float rbf2(const PostArgs &a, long long e, const C3 &c, bool &ok) {
   const bool vd = (c.y + 1 < rows - 1) && ty(a, e + cols) == 0;
   const bool vl = (c.z - 1 >= 1) && ty(a, e - 1) == 0;
   const bool vr = (c.z + 1 < cols - 1) && ty(a, e + 1) == 0;
-  const float u2 = vu ? val<kPassRbf>(a, e, e - 2 * cols) : 0.f;
-  const float d2 = vd ? val<kPassRbf>(a, e, e + 2 * cols) : 0.f;
-  const float l2 = vl ? val<kPassRbf>(a, e, e - 2) : 0.f;
-  const float r2 = vr ? val<kPassRbf>(a, e, e + 2) : 0.f;
+  const float u2 = vu ? valo<kPassRbf>(a, e, c, 0, -2, 0) : 0.f;
+  const float d2 = vd ? valo<kPassRbf>(a, e, c, 0, 2, 0) : 0.f;
+  const float l2 = vl ? valo<kPassRbf>(a, e, c, 0, 0, -2) : 0.f;
+  const float r2 = vr ? valo<kPassRbf>(a, e, c, 0, 0, 2) : 0.f;
   const float step = __fsub_rn(cand, old);
   float alpha = 1.0f;
   for (int it = 0; it < 10; it++) {
@@ -318,18 +349,8 @@ __device__ float rbf2(const PostArgs &a, long long e, const C3 &c, bool &ok) {
 struct Win3 {
   float v[5][5][5];
   unsigned char have[5][5][5];
+  C3 c;  // coordinates of the center
 };
-
-__device__ __forceinline__ float w3get(const PostArgs &a, long long e, Win3 &W, int dx, int dy, int dz,
-                                       float center) {
-  if (dx == 0 && dy == 0 && dz == 0) return center;
-  unsigned char &h = W.have[dx + 2][dy + 2][dz + 2];
-  if (!h) {
-    W.v[dx + 2][dy + 2][dz + 2] = val<kPassRbf>(a, e, e + dx * a.g.plane + dy * a.g.d3 + dz);
-    h = 1;
-  }
-  return W.v[dx + 2][dy + 2][dz + 2];
-}
 
 template <int PASS>
 __device__ __forceinline__ float w3getp(const PostArgs &a, long long e, Win3 &W, int dx, int dy, int dz,
@@ -337,7 +358,7 @@ __device__ __forceinline__ float w3getp(const PostArgs &a, long long e, Win3 &W,
   if (dx == 0 && dy == 0 && dz == 0) return center;
   unsigned char &h = W.have[dx + 2][dy + 2][dz + 2];
   if (!h) {
-    W.v[dx + 2][dy + 2][dz + 2] = val<PASS>(a, e, e + dx * a.g.plane + dy * a.g.d3 + dz);
+    W.v[dx + 2][dy + 2][dz + 2] = valo<PASS>(a, e, W.c, dx, dy, dz);
     h = 1;
   }
   return W.v[dx + 2][dy + 2][dz + 2];
@@ -370,6 +391,7 @@ __device__ bool valid3(const PostArgs &a, long long e, const C3 &c, Win3 &W, flo
 __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
   ok = false;
   Win3 W;
+  W.c = c;
   for (int i = 0; i < 125; i++) (&W.have[0][0][0])[i] = 0;
   const float old = a.F[e];
   double num = 0.0, den = 0.0;
@@ -377,7 +399,7 @@ __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
     for (int db = -1; db <= 1; db++)
       for (int dc = -1; dc <= 1; dc++) {
         double ww = c_w3[(da + 1) * 9 + (db + 1) * 3 + (dc + 1)];
-        if (locked3(a, e + da * a.g.plane + db * a.g.d3 + dc)) ww = __dmul_rn(ww, 0.4);
+        if (locked(a, e + da * a.g.plane + db * a.g.d3 + dc)) ww = __dmul_rn(ww, 0.4);
         const float v = w3getp<kPassRbf>(a, e, W, da, db, dc, old);
         num = __dadd_rn(num, __dmul_rn(ww, (double)v));
         den = __dadd_rn(den, ww);
@@ -405,6 +427,7 @@ __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
 __device__ float axis3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
   ok = false;
   Win3 W;
+  W.c = c;
   for (int i = 0; i < 125; i++) (&W.have[0][0][0])[i] = 0;
   const float old = a.F[e];
   if (cls6_at<kPassAxis>(a, e, W, 0, 0, 0, old) == 3) return old;
@@ -436,114 +459,216 @@ __device__ float axis3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
 }
 
 // ----------------------------------------------------------------------------
-// pass kernel
+// candidate lists
 // ----------------------------------------------------------------------------
-template <int PASS, int ND>
-__global__ void __launch_bounds__(kPostThreads)
-post_pass_kernel(PostArgs a) {
-  __shared__ long long s_tile;
-  __shared__ unsigned s_w[kPostThreads / 32];
-  __shared__ unsigned long long s_base;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long long ntiles = (a.n + kPostTile - 1) / kPostTile;
-  while (true) {
-    if (threadIdx.x == 0) s_tile = (long long)atomicAdd(a.tile_ctr, 1u);
-    __syncthreads();
-    const long long tile = s_tile;
-    if (tile >= ntiles) break;
-    const long long t0 = tile * kPostTile;
-    // candidates of this thread: elements t0 + threadIdx.x*8 + u (contiguous per thread)
-    unsigned cmask = 0;
-    for (int u = 0; u < kPostPer; u++) {
-      const long long e = t0 + (long long)threadIdx.x * kPostPer + u;
-      if (e < a.n && is_cand<PASS>(a, e)) cmask |= 1u << u;
-    }
-    unsigned long long rank0 = 0;
-    if (PASS == kPassStencil) {
-      const unsigned c = __popc(cmask);
-      unsigned incl = c;
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      if (lane == 31) s_w[warp] = incl;
-      __syncthreads();
-      unsigned wpre = 0, ttot = 0;
-      for (int w = 0; w < kPostThreads / 32; w++) { if (w < warp) wpre += s_w[w]; ttot += s_w[w]; }
-      if (warp == 0) {
-        Prefix pf = lookback(a.desc, tile, 0, ttot, a.err);
-        if (lane == 0) s_base = pf.cnt;
-      }
-      __syncthreads();
-      rank0 = s_base + wpre + incl - c;
-    }
-    for (int u = 0; u < kPostPer; u++) {
-      if (!(cmask & (1u << u))) continue;
-      const long long e = t0 + (long long)threadIdx.x * kPostPer + u;
-      const int t = ty(a, e);
-      float r;
-      bool ok = false;
-      if (PASS == kPassStencil) {
-        const int s = (rank0 < a.n_sp) ? a.sp[rank0] : 0;
-        rank0++;
-        r = (ND == 2) ? stencil2(a, e, t, s) : stencil3(a, e, t, s);
-      } else if (PASS == kPassEnforce) {
-        r = enforce<ND>(a, e, t);
-      } else if (PASS == kPassRbf) {
-        const C3 c = coords(a.g, e);
-        r = (ND == 2) ? rbf2(a, e, c, ok) : rbf3(a, e, c, ok);
-      } else {
-        const C3 c = coords(a.g, e);
-        r = axis3(a, e, c, ok);
-      }
-      if (ok) atomicAdd(a.restored, 1u);
-      a.T[e] |= kCandFlag;
-      st_rlx(&a.S[e], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
-    }
-    __syncthreads();
+
+// Interior extrema (list X) and interior saddles (list Z), both in raster
+// order, from the types array: per-tile counts, a scan over the tiles, then a
+// second pass that writes the positions.  Tiles of kPostTile points, 8 per
+// thread; counts packed as (extrema << 32) | saddles.
+__device__ __forceinline__ void tile_masks(const unsigned char *__restrict__ T, const Geom &g, long long n,
+                                           long long i0, unsigned &em, unsigned &sm) {
+  em = 0;
+  sm = 0;
+  if (i0 >= n) return;
+  long long r, x, y, z;
+  if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
+  else { x = fdivmod(i0, g.plane, g.m_plane, r); y = fdivmod(r, g.d3, g.m_d3, z); }
+  unsigned long long w = 0;
+  if (i0 + 8 <= n && ((reinterpret_cast<uintptr_t>(T + i0) & 7) == 0)) {
+    w = *reinterpret_cast<const unsigned long long *>(T + i0);
+  } else {
+    for (int u = 0; u < 8; u++) if (i0 + u < n) w |= (unsigned long long)T[i0 + u] << (8 * u);
+  }
+  if (w == 0) return;
+  for (int u = 0; u < kPostPer; u++) {
+    if (i0 + u >= n) break;
+    bool in = y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
+    if (g.nd == 3) in = in && x >= 1 && x <= g.d1 - 2;
+    const unsigned t = (unsigned)(w >> (8 * u)) & 3u;
+    if (in && (t == 1u || t == 2u)) em |= 1u << u;
+    if (in && t == 3u) sm |= 1u << u;
+    z++;
+    while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
   }
 }
 
-// copy pass results into F and clear the candidate flags
-__global__ void post_scatter_kernel(float *__restrict__ F, unsigned char *__restrict__ T,
-                                    const unsigned long long *__restrict__ S, long long n) {
-  const long long i0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
-  if (i0 >= n) return;
-  if (i0 + 4 <= n && ((reinterpret_cast<uintptr_t>(T + i0) & 3) == 0)) {
-    uint32_t w = *reinterpret_cast<const uint32_t *>(T + i0);
-    if (!(w & 0x80808080u)) return;
-    for (int u = 0; u < 4; u++) {
-      if ((w >> (8 * u)) & 0x80u) {
-        F[i0 + u] = __uint_as_float((unsigned)S[i0 + u]);
-        T[i0 + u] &= 0x7f;
-      }
-    }
-    return;
+__global__ void __launch_bounds__(kPostThreads)
+list_count_kernel(const unsigned char *__restrict__ T, Geom g, long long n, unsigned long long *cnt) {
+  __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
+  const long long i0 = (long long)blockIdx.x * kPostTile + (long long)threadIdx.x * kPostPer;
+  unsigned em, sm;
+  tile_masks(T, g, n, i0, em, sm);
+  unsigned te, ts;
+  cta_excl_scan_post((unsigned)__popc(em), s_w1, &te);
+  cta_excl_scan_post((unsigned)__popc(sm), s_w2, &ts);
+  if (threadIdx.x == 0) cnt[blockIdx.x] = ((unsigned long long)te << 32) | ts;
+}
+
+// exclusive scan of packed tile counts (one CTA of 1024 threads); totals at cnt[ntiles]
+__global__ void list_scan_kernel(unsigned long long *cnt, long long ntiles) {
+  __shared__ unsigned long long part[1024];
+  const long long per = (ntiles + blockDim.x - 1) / blockDim.x;
+  const long long i0 = threadIdx.x * per;
+  unsigned long long sum = 0;
+  for (long long i = 0; i < per; i++) if (i0 + i < ntiles) sum += cnt[i0 + i];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+    const unsigned long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0ull;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
   }
-  for (long long i = i0; i < i0 + 4 && i < n; i++)
-    if (T[i] & 0x80) { F[i] = __uint_as_float((unsigned)S[i]); T[i] &= 0x7f; }
+  unsigned long long run = part[threadIdx.x] - sum;
+  for (long long i = 0; i < per; i++)
+    if (i0 + i < ntiles) { const unsigned long long v = cnt[i0 + i]; cnt[i0 + i] = run; run += v; }
+  if (threadIdx.x == blockDim.x - 1) cnt[ntiles] = part[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kPostThreads)
+list_write_kernel(const unsigned char *__restrict__ T, Geom g, long long n, const unsigned long long *cnt,
+                  unsigned *X, unsigned *Z, unsigned char *Eb, unsigned char *Ib) {
+  __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
+  const long long i0 = (long long)blockIdx.x * kPostTile + (long long)threadIdx.x * kPostPer;
+  unsigned em, sm;
+  tile_masks(T, g, n, i0, em, sm);
+  if (i0 < n) {
+    // interior bits of the 8 points (byte of the interior bitmap)
+    unsigned im = 0;
+    long long r, x, y, z;
+    if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
+    else { x = fdivmod(i0, g.plane, g.m_plane, r); y = fdivmod(r, g.d3, g.m_d3, z); }
+    for (int u = 0; u < kPostPer && i0 + u < n; u++) {
+      bool in = y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
+      if (g.nd == 3) in = in && x >= 1 && x <= g.d1 - 2;
+      if (in) im |= 1u << u;
+      z++;
+      while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
+    }
+    Eb[i0 >> 3] = (unsigned char)em;
+    Ib[i0 >> 3] = (unsigned char)im;
+  }
+  unsigned te, ts;
+  const unsigned eo = cta_excl_scan_post((unsigned)__popc(em), s_w1, &te);
+  const unsigned so = cta_excl_scan_post((unsigned)__popc(sm), s_w2, &ts);
+  const unsigned long long base = cnt[blockIdx.x];
+  unsigned long long xe = (base >> 32) + eo, xs = (base & 0xffffffffull) + so;
+  for (int u = 0; u < kPostPer; u++) {
+    if (em & (1u << u)) X[xe++] = (unsigned)(i0 + u);
+    if (sm & (1u << u)) Z[xs++] = (unsigned)(i0 + u);
+  }
+}
+
+// lost saddles (RBF candidates): saddles of the original field that F no
+// longer classifies as saddles (example/test_cuda_topology.cu:244-254)
+__global__ void fn_detect_kernel(PostArgs a, const unsigned *__restrict__ Z, unsigned long long nz,
+                                 unsigned *__restrict__ R, unsigned *__restrict__ Y, unsigned *y_count) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool lost = false;
+  long long q = 0;
+  if (i < nz) {
+    q = (long long)Z[i];
+    lost = classify_F(a, q) != 3;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, lost);
+  unsigned base = 0;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0 && m) base = atomicAdd(y_count, (unsigned)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (lost) {
+    Y[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)i;
+    atomicOr(&R[q >> 5], 1u << (q & 31));
+  }
+}
+
+// One round of a pass over a worklist of list indices (identity when W is
+// null).  Items whose earlier candidates are not final yet go to Wn.
+template <int PASS, int ND>
+__global__ void __launch_bounds__(kPostThreads)
+pass_round_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *__restrict__ W,
+                  unsigned nw, unsigned *__restrict__ Wn, unsigned *wn_count) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool defer = false;
+  unsigned idx = 0;
+  if (i < nw) {
+    idx = W ? W[i] : i;
+    const long long e = (long long)list[idx];
+    const C3 c = coords(a.g, e);
+    if (!deps_ready<PASS, ND>(a, e, c)) {
+      defer = true;
+    } else {
+      float r;
+      bool ok = false;
+      if (PASS == kPassStencil) {
+        const int t = ty(a, e);
+        const int s = (idx < a.n_sp) ? a.sp[idx] : 0;
+        r = (ND == 2) ? stencil2(a, e, c, t, s) : stencil3(a, e, c, t, s);
+      } else if (PASS == kPassEnforce) {
+        r = enforce<ND>(a, e, c, ty(a, e));
+      } else if (PASS == kPassRbf) {
+        r = (ND == 2) ? rbf2(a, e, c, ok) : rbf3(a, e, c, ok);
+      } else {
+        r = axis3(a, e, c, ok);
+      }
+      if (ok) atomicAdd(a.restored, 1u);
+      st_rlx(&a.S[e], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
+    }
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, defer);
+  const int lane = threadIdx.x & 31;
+  unsigned base = 0;
+  if (lane == 0 && m) base = atomicAdd(wn_count, (unsigned)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (defer) Wn[base + __popc(m & ((1u << lane) - 1u))] = idx;
+}
+
+// F[list[i]] = result of the pass
+__global__ void list_scatter_kernel(float *__restrict__ F, const unsigned long long *__restrict__ S,
+                                    const unsigned *__restrict__ list, unsigned nlist,
+                                    const unsigned *__restrict__ sel) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nlist) return;
+  const long long e = (long long)list[sel ? sel[i] : i];
+  F[e] = __uint_as_float((unsigned)S[e]);
+}
+
+// bits [b, b + 32) of a bitmap of nbits bits (zeros outside)
+__device__ __forceinline__ unsigned get32(const unsigned *__restrict__ bm, long long b, long long nbits) {
+  const long long w = b >> 5;  // arithmetic shift: floor for negative b
+  const unsigned sh = (unsigned)(b & 31);
+  const long long nw = (nbits + 31) >> 5;
+  const unsigned lo = (w >= 0 && w < nw) ? bm[w] : 0u;
+  const unsigned hi = (w + 1 >= 0 && w + 1 < nw) ? bm[w + 1] : 0u;
+  return sh ? __funnelshift_r(lo, hi, sh) : lo;
+}
+
+// lock bitmap: bit q set when q is interior and an interior extremum lies
+// within Chebyshev distance 1 (example/test_cuda_topology.cu:229-242,
+// example/test_cuda_topology_3d.cu:325-341): the interior-extremum bitmap E
+// dilated by one along every axis, masked by the interior bitmap I.  The
+// flat-index offsets of the 3x3(x3) neighbourhood become bit offsets, so each
+// output word ORs 9 (2D) or 27 (3D) shifted 32-bit windows of E.  Points that
+// wrap to another row lie on the boundary and are never interior extrema.
+__global__ void lock_bits_kernel(const unsigned *__restrict__ E, const unsigned *__restrict__ I, Geom g,
+                                 long long n, unsigned *__restrict__ L) {
+  const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nw = (n + 31) >> 5;
+  if (w >= nw) return;
+  const long long b0 = w << 5;
+  unsigned acc = 0;
+  const int xr = (g.nd == 3) ? 1 : 0;
+  for (int da = -xr; da <= xr; da++)
+    for (int db = -1; db <= 1; db++) {
+      const long long o = b0 + (long long)da * g.plane + (long long)db * g.d3;
+      acc |= get32(E, o - 1, n) | get32(E, o, n) | get32(E, o + 1, n);
+    }
+  L[w] = acc & I[w];
 }
 
 __global__ void types_from_int_kernel(const int *__restrict__ fn, unsigned char *__restrict__ T, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) T[i] = (unsigned char)(fn[i] & 3);
-}
-
-template <int PASS, int ND>
-static cudaError_t run_pass(szp_b200_ctx *ctx, PostArgs a, TileDesc *desc, long long ntiles) {
-  cudaStream_t s = ctx->stream;
-  cudaError_t e;
-  if ((e = cudaMemsetAsync(a.tile_ctr, 0, 4, s)) != cudaSuccess) return e;
-  if (PASS == kPassStencil &&
-      (e = cudaMemsetAsync(desc, 0, (ntiles + 1) * sizeof(TileDesc), s)) != cudaSuccess)
-    return e;
-  const int grid = (int)std::min<long long>(ntiles, (long long)ctx->sm_count * 8);
-  post_pass_kernel<PASS, ND><<<grid, kPostThreads, 0, s>>>(a);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const long long sg = (a.n + 4 * 256 - 1) / (4 * 256);
-  post_scatter_kernel<<<(unsigned)sg, 256, 0, s>>>(a.F, a.T, a.S, a.n);
-  ctx->launches += 2;
-  return cudaGetLastError();
 }
 
 static bool g_weights_ready[64];
@@ -568,7 +693,9 @@ static cudaError_t upload_weights(int dev) {
 
 size_t post_scratch_bytes(unsigned long long n) {
   const unsigned long long ntiles = (n + kPostTile - 1) / kPostTile;
-  return a256(n) + a256((ntiles + 1) * sizeof(TileDesc)) + 4096;
+  const unsigned long long words = (n + 31) / 32;
+  // T, descriptors, lock + RBF bitmaps, lists X and Z, worklists (2), Y
+  return a256(n) + a256((ntiles + 1) * sizeof(TileDesc)) + 4 * a256(words * 4 + 4) + 5 * a256(n * 4) + 8192;
 }
 
 // generation counter of the result words (never reused while the buffer lives)
@@ -592,18 +719,161 @@ unsigned long long *post_words(szp_b200_ctx *ctx, unsigned long long n) {
   return ctx->post_S;
 }
 
+// Runs one pass in rounds over `list` (count items); returns 0 on success.
+template <int PASS, int ND>
+static int run_rounds(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, unsigned count,
+                      unsigned *W0, unsigned *W1, const unsigned *sel_for_scatter) {
+  cudaStream_t s = ctx->stream;
+  unsigned *cnt = reinterpret_cast<unsigned *>(ctx->d_words + 7);
+  const unsigned *W = nullptr;  // round 0: every item
+  unsigned nw = count;
+  unsigned *bufs[2] = {W0, W1};
+  int b = 0;
+  for (int round = 0; nw > 0; round++) {
+    if (round > 100000) { set_error("post-processing pass did not converge"); return -1; }
+    if (cuda_fail(cudaMemsetAsync(cnt, 0, 4, s), "memset")) return -1;
+    pass_round_kernel<PASS, ND><<<(nw + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(
+        a, list, W, nw, bufs[b], cnt);
+    ctx->launches += 1;
+    unsigned next = 0;
+    if (cuda_fail(cudaGetLastError(), "pass round") ||
+        cuda_fail(cudaMemcpyAsync(&next, cnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+        cuda_fail(cudaStreamSynchronize(s), "pass round"))
+      return -1;
+    if (next >= nw && round > 0) { set_error("post-processing pass made no progress"); return -1; }
+    W = bufs[b];
+    nw = next;
+    b ^= 1;
+  }
+  if (count) {
+    list_scatter_kernel<<<(count + 255) / 256, 256, 0, s>>>(a.F, a.S, list, count, sel_for_scatter);
+    ctx->launches += 1;
+    if (cuda_fail(cudaGetLastError(), "scatter")) return -1;
+  }
+  return 0;
+}
+
+// rounds over list entries list[sel[i]], i < count (the RBF pass: lost saddles)
+template <int PASS, int ND>
+static int run_rounds_sel(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, const unsigned *sel,
+                          unsigned count, unsigned *W0, unsigned *W1) {
+  cudaStream_t s = ctx->stream;
+  // round 0 runs over sel itself (indices into list)
+  unsigned *cnt = reinterpret_cast<unsigned *>(ctx->d_words + 7);
+  const unsigned *W = sel;
+  unsigned nw = count;
+  unsigned *bufs[2] = {W0, W1};
+  int b = 0;
+  for (int round = 0; nw > 0; round++) {
+    if (round > 100000) { set_error("post-processing pass did not converge"); return -1; }
+    if (cuda_fail(cudaMemsetAsync(cnt, 0, 4, s), "memset")) return -1;
+    pass_round_kernel<PASS, ND><<<(nw + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(
+        a, list, W, nw, bufs[b], cnt);
+    ctx->launches += 1;
+    unsigned next = 0;
+    if (cuda_fail(cudaGetLastError(), "pass round") ||
+        cuda_fail(cudaMemcpyAsync(&next, cnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+        cuda_fail(cudaStreamSynchronize(s), "pass round"))
+      return -1;
+    if (next >= nw && round > 0) { set_error("post-processing pass made no progress"); return -1; }
+    W = bufs[b];
+    nw = next;
+    b ^= 1;
+  }
+  list_scatter_kernel<<<(count + 255) / 256, 256, 0, s>>>(a.F, a.S, list, count, sel);
+  ctx->launches += 1;
+  return cuda_fail(cudaGetLastError(), "scatter") ? -1 : 0;
+}
+
+template <int ND>
+static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned nx, unsigned *Z, unsigned nz,
+                          unsigned *Y, unsigned *W0, unsigned *W1, unsigned *R, unsigned *Lb,
+                          const unsigned *Eb, const unsigned *Ib, int axis_stencil) {
+  cudaStream_t s = ctx->stream;
+  const long long n = a.n;
+  if (a.sp && a.n_sp > 0) {
+    a.gen = next_gen(ctx);
+    if (run_rounds<kPassStencil, ND>(ctx, a, X, nx, W0, W1, nullptr)) return -1;
+    tl_mark(ctx, "post_stencil");
+  }
+  a.gen = next_gen(ctx);
+  if (run_rounds<kPassEnforce, ND>(ctx, a, X, nx, W0, W1, nullptr)) return -1;
+  tl_mark(ctx, "post_enforce");
+  // locks (static: from the types) and the lost saddles (from F after enforcement)
+  const long long words = (n + 31) / 32;
+  lock_bits_kernel<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(Eb, Ib, a.g, n, Lb);
+  if (cuda_fail(cudaMemsetAsync(R, 0, words * 4, s), "memset")) return -1;
+  unsigned *ycnt = reinterpret_cast<unsigned *>(ctx->d_words + 8);
+  if (cuda_fail(cudaMemsetAsync(ycnt, 0, 4, s), "memset")) return -1;
+  a.L = Lb;
+  a.R = R;
+  if (nz) fn_detect_kernel<<<(nz + 255) / 256, 256, 0, s>>>(a, Z, nz, R, Y, ycnt);
+  ctx->launches += 2;
+  unsigned ny = 0;
+  if (cuda_fail(cudaGetLastError(), "fn detect") ||
+      cuda_fail(cudaMemcpyAsync(&ny, ycnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaStreamSynchronize(s), "fn detect"))
+    return -1;
+  tl_mark(ctx, "post_fn_locks");
+  if (ny) {
+    // RBF runs over Z restricted to the lost saddles (Y holds indices into Z)
+    a.gen = next_gen(ctx);
+    if (run_rounds_sel<kPassRbf, ND>(ctx, a, Z, Y, ny, W0, W1)) return -1;
+  }
+  tl_mark(ctx, "post_rbf");
+  if (axis_stencil && ND == 3 && nz) {
+    a.gen = next_gen(ctx);
+    if (run_rounds<kPassAxis, ND>(ctx, a, Z, nz, W0, W1, nullptr)) return -1;
+    tl_mark(ctx, "post_axis");
+  }
+  return 0;
+}
+
 int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsigned char *d_T,
-                     unsigned long long *d_S, TileDesc *desc, const int *d_sp,
+                     unsigned long long *d_S, TileDesc *desc, unsigned *d_L, const int *d_sp,
                      unsigned long long n_sp, const Geom &g, float eb, int axis_stencil,
                      int *restored_out) {
   const long long n = g.d1 * g.d2 * g.d3;
   if (g.d2 < 3 || g.d3 < 3 || (g.nd == 3 && g.d1 < 3)) { if (restored_out) *restored_out = 0; return 0; }
+  if (n >= (1ll << 32)) { set_error("post-processing supports fields of fewer than 2^32 points"); return -1; }
   int dev = 0;
   cudaGetDevice(&dev);
   if (cuda_fail(upload_weights(dev), "weights")) return -1;
   cudaStream_t s = ctx->stream;
+  Arena &A = ctx->scratch;
+  unsigned *X = A.take<unsigned>(n), *Z = A.take<unsigned>(n), *Y = A.take<unsigned>(n);
+  unsigned *W0 = A.take<unsigned>(n), *W1 = A.take<unsigned>(n);
+  unsigned *R = A.take<unsigned>((n + 31) / 32);
+  unsigned *Eb = A.take<unsigned>((n + 31) / 32 + 1), *Ib = A.take<unsigned>((n + 31) / 32 + 1);
+  if (!X || !Z || !Y || !W0 || !W1 || !R || !Eb || !Ib) {
+    set_error("scratch arena too small for post-processing");
+    return -1;
+  }
   unsigned long long *w = ctx->d_words;
-  if (cuda_fail(cudaMemsetAsync(w, 0, 64, s), "memset")) return -1;
+  if (cuda_fail(cudaMemsetAsync(w, 0, 80, s), "memset")) return -1;
+  const long long ntiles = (n + kPostTile - 1) / kPostTile;
+  // per-tile counts live in the descriptor buffer (32 bytes per tile available)
+  unsigned long long *tcnt = reinterpret_cast<unsigned long long *>(desc);
+  {
+    // the words past the last written byte of the two bitmaps must read as zero
+    const long long words = (n + 31) / 32;
+    if (cuda_fail(cudaMemsetAsync(Eb + words - 1, 0, 8, s), "memset") ||
+        cuda_fail(cudaMemsetAsync(Ib + words - 1, 0, 8, s), "memset"))
+      return -1;
+  }
+  list_count_kernel<<<(unsigned)ntiles, kPostThreads, 0, s>>>(d_T, g, n, tcnt);
+  list_scan_kernel<<<1, 1024, 0, s>>>(tcnt, ntiles);
+  list_write_kernel<<<(unsigned)ntiles, kPostThreads, 0, s>>>(d_T, g, n, tcnt, X, Z,
+                                                            reinterpret_cast<unsigned char *>(Eb),
+                                                            reinterpret_cast<unsigned char *>(Ib));
+  ctx->launches += 3;
+  unsigned long long tot = 0;
+  if (cuda_fail(cudaGetLastError(), "lists") ||
+      cuda_fail(cudaMemcpyAsync(&tot, tcnt + ntiles, 8, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaStreamSynchronize(s), "lists"))
+    return -1;
+  const unsigned nx = (unsigned)(tot >> 32), nz = (unsigned)(tot & 0xffffffffull);
+  tl_mark(ctx, "post_lists");
   PostArgs a{};
   a.F = d_data;
   a.O = d_orig;
@@ -616,32 +886,12 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   a.eps = fmaxf(1e-6f, 0.1f * eb);
   a.S = d_S;
   a.desc = desc;
-  a.tile_ctr = reinterpret_cast<unsigned *>(w + 3);
   a.err = reinterpret_cast<int *>(w + 4);
   a.restored = reinterpret_cast<unsigned *>(w + 5);
-  const long long ntiles = (n + kPostTile - 1) / kPostTile;
-  cudaError_t e = cudaSuccess;
-  if (d_sp && n_sp > 0) {
-    a.gen = next_gen(ctx);
-    e = (g.nd == 2) ? run_pass<kPassStencil, 2>(ctx, a, desc, ntiles) : run_pass<kPassStencil, 3>(ctx, a, desc, ntiles);
-    if (cuda_fail(e, "stencil pass")) return -1;
-    tl_mark(ctx, "post_stencil");
-  }
-  a.gen = next_gen(ctx);
-  e = (g.nd == 2) ? run_pass<kPassEnforce, 2>(ctx, a, desc, ntiles) : run_pass<kPassEnforce, 3>(ctx, a, desc, ntiles);
-  if (cuda_fail(e, "enforcement pass")) return -1;
-  tl_mark(ctx, "post_enforce");
-  a.gen = next_gen(ctx);
-  e = (g.nd == 2) ? run_pass<kPassRbf, 2>(ctx, a, desc, ntiles) : run_pass<kPassRbf, 3>(ctx, a, desc, ntiles);
-  if (cuda_fail(e, "rbf pass")) return -1;
-  tl_mark(ctx, "post_rbf");
-  if (axis_stencil && g.nd == 3) {
-    a.gen = next_gen(ctx);
-    e = run_pass<kPassAxis, 3>(ctx, a, desc, ntiles);
-    if (cuda_fail(e, "axis pass")) return -1;
-    tl_mark(ctx, "post_axis");
-  }
-  if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 64, cudaMemcpyDeviceToHost, s), "D2H") ||
+  const int rc = (g.nd == 2) ? run_all_passes<2>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, axis_stencil)
+                             : run_all_passes<3>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, axis_stencil);
+  if (rc) return -1;
+  if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 80, cudaMemcpyDeviceToHost, s), "D2H") ||
       cuda_fail(cudaStreamSynchronize(s), "postprocess"))
     return -1;
   const int err = (int)(ctx->h_words[4] & 0xffffffffu);
@@ -660,7 +910,8 @@ int postprocess(szp_b200_ctx *ctx, float *d_data, const float *d_orig,
   unsigned char *T = A.take<unsigned char>(n);
   const unsigned long long ntiles = (n + kPostTile - 1) / kPostTile;
   TileDesc *desc = A.take<TileDesc>(ntiles + 1);
-  if (!S || !T || !desc) { set_error("scratch arena too small for post-processing"); return -1; }
+  unsigned *Lb = A.take<unsigned>((n + 31) / 32);
+  if (!S || !T || !desc || !Lb) { set_error("scratch arena too small for post-processing"); return -1; }
   cudaStream_t s = ctx->stream;
   if (d_types_i) {
     types_from_int_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_types_i, T, n);
@@ -668,7 +919,7 @@ int postprocess(szp_b200_ctx *ctx, float *d_data, const float *d_orig,
   } else if (cuda_fail(cudaMemcpyAsync(T, d_types_u8, n, cudaMemcpyDeviceToDevice, s), "copy types")) {
     return -1;
   }
-  return postprocess_with(ctx, d_data, d_orig, T, S, desc, d_sp, n_sp, g, eb, axis_stencil, restored_out);
+  return postprocess_with(ctx, d_data, d_orig, T, S, desc, Lb, d_sp, n_sp, g, eb, axis_stencil, restored_out);
 }
 
 }  // namespace tsz

@@ -90,7 +90,97 @@ __global__ void bucket_start_kernel(const unsigned *__restrict__ tot, int NB,
   if (threadIdx.x == blockDim.x - 1) start[NB] = part[threadIdx.x];
 }
 
-// ---- 1d. scatter into buckets ----------------------------------------------
+// ---- 1d. scatter into buckets, coalesced ---------------------------------
+// Each CTA walks its chunk in sub-chunks of kSub records: the records are
+// counting-sorted by bucket in shared memory, then written out in that order,
+// so every bucket's records of a sub-chunk form one contiguous run in global
+// memory (consecutive threads store consecutive addresses).
+constexpr int kSub = 4096;
+constexpr int kScatterThreads = 512;
+
+__global__ void __launch_bounds__(kScatterThreads)
+bucket_scatter_sorted_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
+                             unsigned long long K, float eb, double inv, int logNB,
+                             unsigned long long chunk, const unsigned *__restrict__ M,
+                             const unsigned long long *__restrict__ start, RankRec *__restrict__ recs) {
+  extern __shared__ unsigned char smx[];
+  const int NB = 1 << logNB;
+  unsigned *run = reinterpret_cast<unsigned *>(smx);          // records of this CTA already written per bucket
+  unsigned *hist = run + NB;                                   // per sub-chunk counts
+  unsigned *off = hist + NB;                                   // per sub-chunk exclusive offsets
+  RankRec *stage = reinterpret_cast<RankRec *>(off + NB);      // kSub staged records
+  unsigned short *sb = reinterpret_cast<unsigned short *>(stage + kSub);  // bucket of each staged record
+  __shared__ unsigned s_part[kScatterThreads / 32];
+  for (int b = threadIdx.x; b < NB; b += blockDim.x) run[b] = M[(size_t)blockIdx.x * NB + b];
+  const unsigned long long c0 = blockIdx.x * chunk;
+  const unsigned long long c1 = (c0 + chunk < K) ? c0 + chunk : K;
+  for (unsigned long long sub = c0; sub < c1; sub += kSub) {
+    const int cnt = (int)((c1 - sub) < (unsigned long long)kSub ? (c1 - sub) : kSub);
+    for (int b = threadIdx.x; b < NB; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    // bucket and in-bucket slot of each record (slot order within a bucket is irrelevant)
+    uint2 pr[kSub / kScatterThreads];
+    int bn[kSub / kScatterThreads];
+    unsigned slot[kSub / kScatterThreads];
+#pragma unroll
+    for (int u = 0; u < kSub / kScatterThreads; u++) {
+      const int i = threadIdx.x + u * kScatterThreads;
+      if (i < cnt) {
+        const unsigned long long k = sub + i;
+        pr[u] = pairs[k];
+        bn[u] = rec_bin(pr[u], bins, k, eb, inv);
+        slot[u] = atomicAdd(&hist[(unsigned)bn[u] & (unsigned)(NB - 1)], 1u);
+      }
+    }
+    __syncthreads();
+    // exclusive scan of hist -> off (NB <= 4 * kScatterThreads)
+    {
+      const int per = (NB + kScatterThreads - 1) / kScatterThreads;
+      const int b0 = threadIdx.x * per;
+      unsigned sum = 0;
+      for (int i = 0; i < per; i++) if (b0 + i < NB) sum += hist[b0 + i];
+      unsigned inc = sum;
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+      }
+      if (lane == 31) s_part[warp] = inc;
+      __syncthreads();
+      unsigned wpre = 0;
+      for (int w = 0; w < warp; w++) wpre += s_part[w];
+      unsigned r = wpre + inc - sum;
+      for (int i = 0; i < per; i++)
+        if (b0 + i < NB) { off[b0 + i] = r; r += hist[b0 + i]; }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kSub / kScatterThreads; u++) {
+      const int i = threadIdx.x + u * kScatterThreads;
+      if (i < cnt) {
+        const unsigned b = (unsigned)bn[u] & (unsigned)(NB - 1);
+        const unsigned pos = off[b] + slot[u];
+        RankRec r;
+        r.code = pr[u].x;
+        r.dest = pr[u].y;
+        r.bin = bn[u];
+        stage[pos] = r;
+        sb[pos] = (unsigned short)b;
+      }
+    }
+    __syncthreads();
+    // write in staged (bucket) order: global = start[b] + run[b] + (pos - off[b])
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const unsigned b = sb[i];
+      recs[start[b] + run[b] + (unsigned)(i - off[b])] = stage[i];
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < NB; b += blockDim.x) run[b] += hist[b];
+    __syncthreads();
+  }
+}
+
+// ---- 1d'. scatter into buckets (unsorted, kept for reference sizes) -------
 __global__ void bucket_scatter_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
                                       unsigned long long K, float eb, double inv, int logNB,
                                       unsigned long long chunk, const unsigned *__restrict__ M,
@@ -141,41 +231,36 @@ bucket_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *_
   const unsigned long long r0 = start[b], r1 = start[b + 1];
   if (r1 == r0) return;
   const unsigned long long cnt = r1 - r0;
+  // bins of this bucket are b + k * NB; slot = k mod kMaxSlots is one-to-one
+  // whenever the bucket's bins span fewer than kMaxSlots values of k
+  for (int sl = threadIdx.x; sl < kMaxSlots; sl += blockDim.x) { s_min[sl] = 0xffffffffu; s_max[sl] = 0u; }
   if (threadIdx.x == 0) { s_bmin = 0x7fffffff; s_bmax = (int)0x80000000; s_fail = 0; }
   __syncthreads();
   int lmin = 0x7fffffff, lmax = (int)0x80000000;
   for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const int bin = recs[r0 + i].bin;
-    lmin = min(lmin, bin);
-    lmax = max(lmax, bin);
+    const RankRec r = recs[r0 + i];
+    lmin = min(lmin, r.bin);
+    lmax = max(lmax, r.bin);
+    const int sl = (r.bin >> logNB) & (kMaxSlots - 1);
+    atomicMin(&s_min[sl], r.code);
+    atomicMax(&s_max[sl], r.code);
   }
   atomicMin(&s_bmin, lmin);
   atomicMax(&s_bmax, lmax);
   __syncthreads();
-  const long long span = ((long long)s_bmax - (long long)s_bmin) >> logNB;
+  const long long span = ((long long)s_bmax >> logNB) - ((long long)s_bmin >> logNB);
   if (span + 1 > kMaxSlots) {
     if (threadIdx.x == 0) fb_list[atomicAdd(fb_count, 1u)] = b;
     return;
   }
-  const int nslots = (int)span + 1;
-  for (int s = threadIdx.x; s < nslots; s += blockDim.x) { s_min[s] = 0xffffffffu; s_max[s] = 0u; }
-  __syncthreads();
-  const int bmin = s_bmin;
-  for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const RankRec r = recs[r0 + i];
-    const int s = (int)(((long long)r.bin - bmin) >> logNB);
-    atomicMin(&s_min[s], r.code);
-    atomicMax(&s_max[s], r.code);
-  }
-  __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long w = 0;
-    for (int s = 0; s < nslots; s++) {
-      s_wbase[s] = (unsigned)w;
-      if (s_max[s] >= s_min[s]) w += ((s_max[s] - s_min[s]) >> 5) + 1;
+    for (int sl = 0; sl < kMaxSlots; sl++) {
+      s_wbase[sl] = (unsigned)w;
+      if (s_max[sl] >= s_min[sl]) w += ((s_max[sl] - s_min[sl]) >> 5) + 1;
       if (w > kBitmapWords) { s_fail = 1; break; }
     }
-    s_wbase[nslots] = (unsigned)w;
+    s_wbase[kMaxSlots] = (unsigned)w;
     s_total_words = (unsigned)w;
   }
   __syncthreads();
@@ -188,19 +273,19 @@ bucket_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *_
   __syncthreads();
   for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
     const RankRec r = recs[r0 + i];
-    const int s = (int)(((long long)r.bin - bmin) >> logNB);
-    const unsigned pos = r.code - s_min[s];
-    atomicOr(&bm[s_wbase[s] + (pos >> 5)], 1u << (pos & 31));
+    const int sl = (r.bin >> logNB) & (kMaxSlots - 1);
+    const unsigned pos = r.code - s_min[sl];
+    atomicOr(&bm[s_wbase[sl] + (pos >> 5)], 1u << (pos & 31));
   }
   __syncthreads();
   // exclusive prefix popcount over the bitmap words (each thread owns a run)
   {
     const unsigned per = (W + blockDim.x - 1) / blockDim.x;
     const unsigned w0 = threadIdx.x * per;
-    unsigned s = 0;
-    for (unsigned i = 0; i < per; i++) if (w0 + i < W) s += __popc(bm[w0 + i]);
+    unsigned sm = 0;
+    for (unsigned i = 0; i < per; i++) if (w0 + i < W) sm += __popc(bm[w0 + i]);
     __shared__ unsigned part[kRankThreads];
-    part[threadIdx.x] = s;
+    part[threadIdx.x] = sm;
     __syncthreads();
     for (int o = 1; o < (int)blockDim.x; o <<= 1) {
       unsigned v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0u;
@@ -208,7 +293,7 @@ bucket_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *_
       part[threadIdx.x] += v;
       __syncthreads();
     }
-    unsigned run = part[threadIdx.x] - s;
+    unsigned run = part[threadIdx.x] - sm;
     for (unsigned i = 0; i < per; i++)
       if (w0 + i < W) { pref[w0 + i] = run; run += __popc(bm[w0 + i]); }
   }
@@ -216,11 +301,11 @@ bucket_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *_
   for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
     const RankRec r = recs[r0 + i];
     if (r.dest == kNoExtremum) continue;
-    const int s = (int)(((long long)r.bin - bmin) >> logNB);
-    const unsigned pos = r.code - s_min[s];
-    const unsigned w = s_wbase[s] + (pos >> 5);
+    const int sl = (r.bin >> logNB) & (kMaxSlots - 1);
+    const unsigned pos = r.code - s_min[sl];
+    const unsigned w = s_wbase[sl] + (pos >> 5);
     const unsigned below = __popc(bm[w] & ((1u << (pos & 31)) - 1u));
-    out[r.dest] = (int)(pref[w] - pref[s_wbase[s]] + below);
+    out[r.dest] = (int)(pref[w] - pref[s_wbase[sl]] + below);
   }
 }
 
@@ -377,8 +462,10 @@ int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
   if (K == 0) return 0;
   cudaStream_t s = ctx->stream;
   const double inv = 1.0 / (double)eb;
+  // 2^9 buckets keep each bucket's bins (slots) within the shared bitmap for
+  // typical fields while giving the coalesced scatter long runs
   int logNB = 6;
-  while (logNB < 14 && (K >> logNB) > 2048) logNB++;
+  while (logNB < 9 && (K >> logNB) > 2048) logNB++;
   const int NB = 1 << logNB;
   int G = ctx->sm_count * 2;
   unsigned long long chunk = (K + G - 1) / G;
@@ -400,7 +487,12 @@ int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
   bucket_hist_kernel<<<G, 512, hsm, s>>>(d_pairs, d_bins, K, eb, inv, logNB, chunk, M);
   bucket_colscan_kernel<<<(NB + 255) / 256, 256, 0, s>>>(M, G, NB, tot);
   bucket_start_kernel<<<1, 1024, 0, s>>>(tot, NB, start);
-  bucket_scatter_kernel<<<G, 512, hsm, s>>>(d_pairs, d_bins, K, eb, inv, logNB, chunk, M, start, recs);
+  {
+    const size_t ssm = (size_t)3 * NB * 4 + (size_t)kSub * sizeof(RankRec) + (size_t)kSub * 2 + 64;
+    cudaFuncSetAttribute(bucket_scatter_sorted_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm);
+    bucket_scatter_sorted_kernel<<<G, kScatterThreads, ssm, s>>>(d_pairs, d_bins, K, eb, inv, logNB, chunk, M,
+                                                                 start, recs);
+  }
   if (cuda_fail(cudaMemsetAsync(fb_cnt, 0, 16, s), "memset")) return -1;
   bucket_rank_kernel<<<NB, kRankThreads, 0, s>>>(recs, start, logNB, d_sp, fb_list, fb_cnt);
   ctx->launches += 5;
@@ -451,7 +543,7 @@ int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
 
 size_t rank_scratch_bytes(unsigned long long K, int sm_count) {
   int logNB = 6;
-  while (logNB < 14 && (K >> logNB) > 2048) logNB++;
+  while (logNB < 9 && (K >> logNB) > 2048) logNB++;
   const size_t NB = (size_t)1 << logNB;
   const size_t G = (size_t)sm_count * 2 + 1;
   // fallback worst case: all K records (two key/value ping-pong buffers + histogram)
