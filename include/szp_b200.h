@@ -198,6 +198,25 @@ SZP_B200_API int szp_b200_topo_postprocess_dev(szp_b200_ctx *ctx, float *d_data,
                                   const int *d_types, const int *d_sp, size_t n_sp,
                                   szp_b200_geom geom, float absErrBound, int axis_stencil);
 
+/* Topology stream of a device-resident field without any allocation (no
+ * counterpart in the reference).  For callers that may not let a library
+ * allocate device memory: code inside a framework that owns every device
+ * allocation, and latency-critical paths where cudaMalloc/cudaFree would
+ * synchronise the device.  Writes the same bytes as the topology stream of
+ * szp_b200_topo_compress_dev (header included) into d_topo (topo_cap bytes,
+ * szp_b200_topo_bound(n, B) always suffices) and its length to *topo_bytes.
+ * Its only scratch is a fixed 4 MiB device array inside the library: fields
+ * needing more than 131072 tile descriptors (more than 268,435,456 elements
+ * at blockSize 64) are rejected with an error.  The first call on each
+ * device resolves that array's address; make it before any stream capture
+ * begins.  Calls on one device share the array: overlapping calls race, so
+ * serialise them.  Synchronous on cuda_stream (0 = legacy default stream).
+ * Returns 0 on success, -1 with szp_b200_last_error() set otherwise. */
+SZP_B200_API int szp_b200_topo_encode_noalloc(const float *d_data, szp_b200_geom geom,
+                                 float absErrBound, int blockSize,
+                                 unsigned char *d_topo, size_t topo_cap,
+                                 size_t *topo_bytes, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

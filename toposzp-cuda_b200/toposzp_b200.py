@@ -48,6 +48,7 @@ EXPORTS = [
     "szp_b200_ctx_launches",
     "szp_b200_topo_compress_host",
     "szp_b200_topo_decompress_host",
+    "szp_b200_topo_encode_noalloc",
 ]
 
 
@@ -108,6 +109,7 @@ def lib():
             "szp_b200_ctx_launches": (C.c_ulonglong, [vp]),
             "szp_b200_topo_compress_host": (i, [vp, vp, Geom, f, i, vp, sz, vp, sz, C.POINTER(Sizes)]),
             "szp_b200_topo_decompress_host": (i, [vp, vp, sz, vp, sz, Geom, f, i, vp, i]),
+            "szp_b200_topo_encode_noalloc": (i, [vp, Geom, f, i, vp, sz, C.POINTER(sz), vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -239,6 +241,19 @@ def geom_of(shape) -> Geom:
     for i, v in enumerate(shape):
         g.dims[i] = int(v)
     return g
+
+
+def encode_noalloc(d_data, shape, eb: float, block_size: int, d_topo, stream_handle: int = 0) -> int:
+    """Topology stream of a device field into the caller's uint8 device
+    tensor d_topo, with no allocation inside the library; returns the stream
+    length in bytes.  Calls on one device must not overlap."""
+    nbytes = C.c_size_t(0)
+    rc = lib().szp_b200_topo_encode_noalloc(
+        C.c_void_p(d_data.data_ptr()), geom_of(shape), eb, block_size, C.c_void_p(d_topo.data_ptr()),
+        d_topo.numel(), C.byref(nbytes), C.c_void_p(stream_handle) if stream_handle else None)
+    if rc:
+        raise ToposzpError(last_error())
+    return int(nbytes.value)
 
 
 class Context:
