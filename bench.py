@@ -51,25 +51,68 @@ def peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples SM clocks and clock-event (throttle) reasons during the timed
+    region: NVML polled every 10 ms from a thread (the GPU is matched by UUID),
+    else nvidia-smi at its 100 ms minimum interval."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+    def __init__(self, device_index: int, period_s: float = 0.01):
+        self.dev = device_index
+        self.period = period_s
+        self.samples = []          # (sm_mhz, reason_bits)
+        self.sm_max = None
+        self.source = None
         self.proc = None
         self.lines = []
+        self._stop = threading.Event()
+        self._nvml = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        self._nvml = pynvml
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _poll(self, h):
+        N = self._nvml
+        while not self._stop.is_set():
+            try:
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                bits = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), int(bits)))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
         try:
+            h = self._nvml_handle()
+            self.sm_max = float(self._nvml.nvmlDeviceGetMaxClockInfo(h, self._nvml.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, args=(h,), daemon=True)
+            self.t.start()
+            self.source = "nvml"
+            return self
+        except Exception:
+            pass
+        try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.source = "nvidia-smi"
         except Exception:
             self.proc = None
         return self
@@ -79,6 +122,9 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self._stop.set()
+        if self.source == "nvml":
+            self.t.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -87,22 +133,30 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
+        sm, reasons = [], set()
+        mx = self.sm_max
+        if self.source == "nvml":
+            for mhz, bits in self.samples:
+                sm.append(mhz)
+                for b, nm in self.REASONS.items():
+                    if bits & b:
+                        reasons.add(nm)
+        else:
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for ln in self.lines:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": self.source}
 
 
 def dist_setup(n_gpus):
@@ -194,7 +248,7 @@ def reference_leg(f, planes, threads):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--side", type=int, default=512, help="edge of the cubic field")
@@ -256,7 +310,9 @@ def main():
     n = f.n
     d_field = torch.from_numpy(f.data.reshape(-1)).to(dev)
 
-    ctx = T.Context(torch.cuda.current_stream(dev).cuda_stream)
+    # the library runs on this stream; every CUDA event below is recorded on it
+    stream = torch.cuda.Stream(device=dev)
+    ctx = T.Context(stream.cuda_stream)
     L = T.lib()
     topo = torch.empty(L.szp_b200_topo_bound(n, B), dtype=torch.uint8, device=dev)
     sort = torch.empty(L.szp_b200_sort_bound(n, B), dtype=torch.uint8, device=dev)
@@ -287,7 +343,6 @@ def main():
     l0 = ctx.launches()
     barrier(world)
     torch.cuda.synchronize()
-    stream = torch.cuda.current_stream(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         ev0.record(stream)
@@ -343,7 +398,7 @@ def main():
         h_sort = torch.empty(L.szp_b200_sort_bound(n, B), dtype=torch.uint8).pin_memory()
         h_out = torch.empty(dims, dtype=torch.float32).pin_memory()
         hf, ht, hs, ho = (h_field.numpy(), h_topo.numpy(), h_sort.numpy(), h_out.numpy())
-        ectx = T.Context(torch.cuda.current_stream(dev).cuda_stream)
+        ectx = T.Context(stream.cuda_stream)
 
         def e2e_step():
             sz = ectx.compress_host(hf, eb, B, ht, hs)
@@ -361,13 +416,14 @@ def main():
             sz = e2e_step()
         e1.record(stream)
         torch.cuda.synchronize()
+        wall_ms = (time.perf_counter() - t0) * 1e3 / ke
         e_ms = max_over_ranks(e0.elapsed_time(e1) / ke, world)
         same = bool(np.array_equal(ho.reshape(-1).view(np.int32), out.cpu().numpy().view(np.int32)))
         e2e = {"value": world * 4.0 * n / (e_ms * 1e-3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": 4 * n + sz.topo_bytes + sz.sort_bytes,
                "d2h_bytes_per_step": sz.topo_bytes + sz.sort_bytes + 4 * n,
                "ms_per_step": e_ms, "matches_device_path": same,
-               "wall_ms_per_step": (time.perf_counter() - t0) * 1e3 / ke}
+               "wall_ms_per_step": wall_ms}
         ectx.close()
 
     cpu = None

@@ -187,3 +187,99 @@ def test_errors_do_not_exit(T):
         T.compress_topology(d, 1e-3, 300, np.zeros(0, dtype=T.CP2_DT))
     with pytest.raises(T.ToposzpError):
         T.compress_topology(d, -1.0, 64, np.zeros(0, dtype=T.CP2_DT))
+
+
+def _oracle_round_trip(ora, d, dims, eb, B):
+    ocp = ora.sort_cp(ora.find_cp(d, eb), d)
+    s_ora = ora.encode_topo(d, eb, B, ora.mark_types(ocp, dims))
+    sp = ora.extract_sp(ocp)
+    s_sp = ora.encode_ints(sp, B) if len(sp) else b""
+    oraw, ofn, _ = ora.decode_topo(s_ora, d.size, eb, B)
+    ref, _ = ora.post(oraw.reshape(dims), oraw.reshape(dims), ofn.reshape(dims), sp, eb)
+    return s_ora, s_sp, oraw, ref
+
+
+def _dev_bytes(b):
+    import torch
+    return torch.from_numpy(np.frombuffer(b, dtype=np.uint8).copy()).cuda() if b else None
+
+
+@pytest.mark.parametrize("case", CASES_2D + CASES_3D, ids=lambda c: "x".join(map(str, c[0])) + "_B%d" % c[2])
+def test_device_parse_and_host_buffers(T, ora, case):
+    """Streams without a block index (offsets parsed on the device) and the
+    host-buffer entry points give the oracle's bytes and values."""
+    dims, eb, B, kind, scale = case
+    d = field(dims, kind, scale)
+    s_ora, s_sp, oraw, ref = _oracle_round_trip(ora, d, dims, eb, B)
+    ctx = T.Context()
+    dt, ds = _dev_bytes(s_ora), _dev_bytes(s_sp)
+    raw = ctx.decompress(dt, len(s_ora), ds, len(s_sp), None, dims, eb, B, postprocess=0)
+    assert (bits(raw.cpu().numpy()) == bits(oraw)).all()
+    post = ctx.decompress(dt, len(s_ora), ds, len(s_sp), None, dims, eb, B, postprocess=1)
+    assert (bits(post.cpu().numpy()) == bits(ref.reshape(-1))).all()
+    n = d.size
+    L = T.lib()
+    h_topo = np.zeros(L.szp_b200_topo_bound(n, B), dtype=np.uint8)
+    h_sort = np.zeros(L.szp_b200_sort_bound(n, B), dtype=np.uint8)
+    sz = ctx.compress_host(d, eb, B, h_topo, h_sort)
+    assert h_topo[: sz.topo_bytes].tobytes() == s_ora
+    assert h_sort[: sz.sort_bytes].tobytes() == s_sp
+    out = np.full(dims, np.nan, dtype=np.float32)
+    ctx.decompress_host(h_topo, sz.topo_bytes, h_sort, sz.sort_bytes, dims, eb, B, out, 1)
+    assert (bits(out) == bits(ref)).all()
+    ctx.close()
+
+
+def test_device_parse_many_segments(T, ora):
+    """A stream long enough for three composition levels of the parser."""
+    import torch
+    dims, eb, B = (96, 128, 160), 1e-4, 64
+    d = synth.small_field(dims, seed=9, kind="band")
+    ctx = T.Context()
+    dd = torch.from_numpy(d.reshape(-1).copy()).cuda()
+    topo, sort, idx, sizes = ctx.compress(dd, dims, eb, B)
+    assert sizes.topo_bytes > 32 * 16384
+    a = ctx.decompress(topo, sizes.topo_bytes, sort, sizes.sort_bytes, idx, dims, eb, B, postprocess=1)
+    b = ctx.decompress(topo, sizes.topo_bytes, sort, sizes.sort_bytes, None, dims, eb, B, postprocess=1)
+    assert torch.equal(a.view(torch.int32), b.view(torch.int32))
+    ctx.close()
+
+
+def test_truncated_stream_is_an_error(T, ora):
+    dims, eb, B = (60, 90), 1e-2, 16
+    d = field(dims, "bumps", 1.0)
+    s_ora, s_sp, _, _ = _oracle_round_trip(ora, d, dims, eb, B)
+    ctx = T.Context()
+    cut = s_ora[: len(s_ora) - 5]
+    with pytest.raises(T.ToposzpError):
+        ctx.decompress(_dev_bytes(cut), len(cut), _dev_bytes(s_sp), len(s_sp), None, dims, eb, B,
+                       postprocess=0)
+    h = np.frombuffer(cut, dtype=np.uint8).copy()
+    out = np.zeros(dims, dtype=np.float32)
+    with pytest.raises(T.ToposzpError):
+        ctx.decompress_host(h, len(cut), np.frombuffer(s_sp, np.uint8).copy(), len(s_sp), dims, eb, B,
+                            out, 1)
+    ctx.close()
+
+
+def test_host_decompress_two_chunk_table(T, ora):
+    """A stream with a two-entry offset table (the reference's OpenMP layout)
+    is detected on the host, as the reference decoder does."""
+    import torch
+    dims, eb, B = (60, 90), 1e-2, 16
+    d = field(dims, "bumps", 1.0)
+    s_ora, s_sp, oraw, ref = _oracle_round_trip(ora, d, dims, eb, B)
+    ctx = T.Context()
+    dd = torch.from_numpy(d.reshape(-1).copy()).cuda()
+    _, _, idx, _ = ctx.compress(dd, dims, eb, B)
+    nb = (d.size + B - 1) // B
+    bpt = (nb + 1) // 2
+    off1 = int(idx[bpt].item())
+    s2 = np.zeros(8, np.uint8).tobytes() + np.array([off1], dtype="<u8").tobytes() + s_ora[8:]
+    oraw2, _, _ = ora.decode_topo(s2, d.size, eb, B)
+    assert (bits(oraw2) == bits(oraw)).all()
+    out = np.zeros(dims, dtype=np.float32)
+    ctx.decompress_host(np.frombuffer(s2, np.uint8).copy(), len(s2), np.frombuffer(s_sp, np.uint8).copy(),
+                        len(s_sp), dims, eb, B, out, 1)
+    assert (bits(out) == bits(ref)).all()
+    ctx.close()

@@ -137,14 +137,19 @@ static bool span_one(const unsigned char *s, unsigned long long pos, unsigned lo
 
 // Fills per-block payload offsets (relative to the end of the offset table);
 // returns false on a malformed stream.
+// buf_len bounds every read when the caller knows the stream length (the
+// reference interface does not: ~0 then, as in the reference).
 static bool walk_stream(const unsigned char *s, unsigned long long n, int B, bool tags,
                         std::vector<unsigned long long> &offs, unsigned long long &hdr,
-                        unsigned long long &payload_len) {
+                        unsigned long long &payload_len, unsigned long long buf_len = ~0ull) {
   const unsigned long long nb = (n + B - 1) / B;
-  const unsigned long long maxc = tags ? 8ull * n + 1024 : 4ull * n + 4;
+  const unsigned long long maxc = std::min<unsigned long long>(tags ? 8ull * n + 1024 : 4ull * n + 4, buf_len);
+  const bool bounded = buf_len != ~0ull;
+  if (buf_len < 8) return false;
   unsigned T = 1;
   if (rd64(s) == 0) {
     for (unsigned t = 1; t <= 128; t++) {
+      if (8ull * t > buf_len) break;
       bool ok = true;
       for (unsigned k = 1; k < t; k++) {
         unsigned long long a = rd64(s + 8 * k), b = rd64(s + 8 * (k - 1));
@@ -195,14 +200,14 @@ static bool walk_stream(const unsigned char *s, unsigned long long n, int B, boo
         unsigned long long b1 = std::min<unsigned long long>((c + 1) * bpt, nb);
         for (unsigned long long b = c * bpt; b < b1; b++) {
           unsigned long long e0 = b * B, m = std::min<unsigned long long>(B, n - e0);
-          if (!span_one(s, pos, 0, m, true, false, &pos)) { overlap = true; break; }
+          if (!span_one(s, pos, buf_len, m, true, bounded, &pos)) { overlap = true; break; }
         }
       } else {
         const unsigned long long tbs = n / T;
         unsigned long long lo = c * tbs, hi = (c == T - 1) ? n : (c + 1) * tbs;
         for (unsigned long long i = lo; i < hi; i += B) {
           unsigned long long m = std::min<unsigned long long>(B, hi - i);
-          if (!span_one(s, pos, 0, m, false, false, &pos)) { overlap = true; break; }
+          if (!span_one(s, pos, buf_len, m, false, bounded, &pos)) { overlap = true; break; }
         }
       }
       prev_end = pos;
@@ -220,7 +225,7 @@ static bool walk_stream(const unsigned char *s, unsigned long long n, int B, boo
       for (unsigned long long b = c * bpt; b < b1; b++) {
         unsigned long long e0 = b * B, m = std::min<unsigned long long>(B, n - e0);
         offs[b] = pos - hdr;
-        if (!span_one(s, pos, 0, m, true, false, &pos)) return false;
+        if (!span_one(s, pos, buf_len, m, true, bounded, &pos)) return false;
         if (pos > end) end = pos;
       }
     }
@@ -233,7 +238,7 @@ static bool walk_stream(const unsigned char *s, unsigned long long n, int B, boo
       for (unsigned long long i = lo; i < hi && b < nb; i += B, b++) {
         unsigned long long m = std::min<unsigned long long>(B, hi - i);
         offs[b] = pos - hdr;
-        if (!span_one(s, pos, 0, m, false, false, &pos)) return false;
+        if (!span_one(s, pos, buf_len, m, false, bounded, &pos)) return false;
         if (pos > end) end = pos;
       }
     }
@@ -574,18 +579,22 @@ int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_data, szp_b200_
   return 0;
 }
 
-int szp_b200_topo_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_topo, size_t topo_bytes,
-                                 const unsigned char *d_sort, size_t sort_bytes,
-                                 const uint64_t *d_blk_index, szp_b200_geom geom, float absErrBound,
-                                 int blockSize, float *d_out, unsigned char *d_types,
-                                 int postprocess) {
-  clear_error();
+}  // extern "C"
+
+namespace tsz {
+
+// Fused decompression (+ post-processing) of device-resident streams.  With
+// d_blk_index == nullptr the block offsets of both streams are parsed on the
+// device; ref_bound selects the reference's validation bound for that parse
+// and *parse_failed reports a stream that is not a valid single-chunk stream.
+static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, size_t topo_bytes,
+                               const unsigned char *d_sort, size_t sort_bytes,
+                               const uint64_t *d_blk_index, szp_b200_geom geom, float absErrBound,
+                               int blockSize, float *d_out, unsigned char *d_types, int postprocess,
+                               bool ref_bound, bool *parse_failed) {
+  if (parse_failed) *parse_failed = false;
   if (!ctx || !d_topo || !d_out) { set_error("null argument"); return -1; }
   if (!check_block_size(blockSize, "szp_b200_topo_decompress_dev")) return -1;
-  if (!d_blk_index) {
-    set_error("szp_b200_topo_decompress_dev: a block index from szp_b200_topo_compress_dev is required");
-    return -1;
-  }
   if (topo_bytes < 8) { set_error("topology stream too short"); return -1; }
   unsigned long long n;
   Geom g;
@@ -593,19 +602,32 @@ int szp_b200_topo_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_topo,
   const int B = blockSize;
   const unsigned long long nb = (n + B - 1) / B;
   const bool post = postprocess != 0;
-  const size_t need = (post ? a256(n * 4) + post_scratch_bytes(n) + a256(n * 4) : 0) + a256(n) + 8192;
+  const bool parse = d_blk_index == nullptr;
+  const bool have_sort = d_sort && sort_bytes > 8;
+  size_t need = (post ? a256(n * 4) + post_scratch_bytes(n) + a256(n * 4) : 0) + a256(n) + 8192;
+  if (parse)
+    need += a256(2 * nb * 8) + parse_scratch_bytes(topo_bytes - 8, B, true) +
+            (post && have_sort ? parse_scratch_bytes(sort_bytes - 8, B, false) : 0);
   if (!ctx->scratch.reserve(need)) return -1;
   Arena &A = ctx->scratch;
   float *O = post ? A.take<float>(n) : nullptr;
   int *sp = post ? A.take<int>(n) : nullptr;
   unsigned char *T = d_types ? d_types : A.take<unsigned char>(n);
+  unsigned long long *idx = parse ? A.take<unsigned long long>(2 * nb)
+                                  : reinterpret_cast<unsigned long long *>(const_cast<uint64_t *>(d_blk_index));
   cudaStream_t s = ctx->stream;
-  unsigned long long *w = ctx->d_words;
+  unsigned long long *w = ctx->d_words;  // [16..17] topology parse status, [18..19] sort parse status
   if (cuda_fail(cudaMemsetAsync(w, 0, 64, s), "memset")) return -1;
+  tl_begin(ctx);
+  if (parse) {
+    if (parse_stream(ctx, A, d_topo + 8, topo_bytes - 8, n, nullptr, B, true, ref_bound, idx, w + 16))
+      return -1;
+    tl_mark(ctx, "parse_topo");
+  }
   DecArgs a{};
   a.payload = d_topo + 8;
   a.payload_len = topo_bytes - 8;
-  a.blk_off = reinterpret_cast<const unsigned long long *>(d_blk_index);
+  a.blk_off = idx;
   a.n = n;
   a.B = B;
   a.eb = absErrBound;
@@ -613,25 +635,43 @@ int szp_b200_topo_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_topo,
   a.fn_u8 = T;
   a.err = reinterpret_cast<int *>(w + 4);
   a.ext_count = w + 6;
-  tl_begin(ctx);
   if (cuda_fail(launch_decode(true, a, s), "decode")) return -1;
   ctx->launches += 1;
   tl_mark(ctx, "decode_topo");
   if (post && cuda_fail(cudaMemcpyAsync(O, d_out, n * 4, cudaMemcpyDeviceToDevice, s), "copy"))
     return -1;
   if (post) tl_mark(ctx, "copy_orig");
-  if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 64, cudaMemcpyDeviceToHost, s), "D2H") ||
+  if (parse && post && have_sort) {
+    // the sort stream holds one value per extremum: its element count is the
+    // decoder's count of type-1/2 tags, read on the device
+    if (parse_stream(ctx, A, d_sort + 8, sort_bytes - 8, 0, w + 6, B, false, ref_bound, idx + nb, w + 18))
+      return -1;
+    tl_mark(ctx, "parse_sort");
+  }
+  if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 20 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+                "D2H") ||
       cuda_fail(cudaStreamSynchronize(s), "decode"))
     return -1;
+  if (parse && (ctx->h_words[16] == 0 || ctx->h_words[17] != 0)) {
+    if (parse_failed) *parse_failed = true;
+    set_error("topology stream is not a valid single-chunk stream (pass the block index from "
+              "szp_b200_topo_compress_dev, or use the host-buffer entry point)");
+    return -1;
+  }
   if (ctx->h_words[4] & 0xffffffffu) { set_error("decoder reported malformed stream"); return -1; }
   if (!post) return 0;
   const unsigned long long E = ctx->h_words[6];
   const int *spp = nullptr;
-  if (E > 0 && d_sort && sort_bytes > 8) {
+  if (E > 0 && have_sort) {
+    if (parse && (ctx->h_words[18] == 0 || ctx->h_words[19] != 0)) {
+      if (parse_failed) *parse_failed = true;
+      set_error("sort-position stream is not a valid single-chunk stream");
+      return -1;
+    }
     DecArgs b{};
     b.payload = d_sort + 8;
     b.payload_len = sort_bytes - 8;
-    b.blk_off = reinterpret_cast<const unsigned long long *>(d_blk_index) + nb;
+    b.blk_off = idx + nb;
     b.n = E;
     b.B = B;
     b.out_i = sp;
@@ -649,6 +689,20 @@ int szp_b200_topo_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_topo,
   int restored = 0;
   return postprocess_with(ctx, d_out, O, T, S, desc, Lb, spp, spp ? E : 0, g, absErrBound,
                           postprocess == 2, &restored);
+}
+
+}  // namespace tsz
+
+extern "C" {
+
+int szp_b200_topo_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_topo, size_t topo_bytes,
+                                 const unsigned char *d_sort, size_t sort_bytes,
+                                 const uint64_t *d_blk_index, szp_b200_geom geom, float absErrBound,
+                                 int blockSize, float *d_out, unsigned char *d_types,
+                                 int postprocess) {
+  clear_error();
+  return decompress_dev_impl(ctx, d_topo, topo_bytes, d_sort, sort_bytes, d_blk_index, geom, absErrBound,
+                             blockSize, d_out, d_types, postprocess, false, nullptr);
 }
 
 int szp_b200_topo_postprocess_dev(szp_b200_ctx *ctx, float *d_data, const float *d_orig,
@@ -772,12 +826,12 @@ int szp_b200_topo_compress_host(szp_b200_ctx *ctx, const float *h_data, szp_b200
   return 0;
 }
 
-int szp_b200_topo_decompress_host(szp_b200_ctx *ctx, const unsigned char *h_topo, size_t topo_bytes,
-                                  const unsigned char *h_sort, size_t sort_bytes, szp_b200_geom geom,
-                                  float absErrBound, int blockSize, float *h_out, int postprocess) {
-  clear_error();
-  if (!ctx || !h_topo || !h_out) { set_error("null argument"); return -1; }
-  if (!check_block_size(blockSize, "szp_b200_topo_decompress_host")) return -1;
+// Host-walk form: the reference's thread-count detection and serial block
+// walk on the host (multi-chunk offset tables and the other cases the device
+// parser leaves to it).
+static int decompress_host_walk(szp_b200_ctx *ctx, const unsigned char *h_topo, size_t topo_bytes,
+                                const unsigned char *h_sort, size_t sort_bytes, szp_b200_geom geom,
+                                float absErrBound, int blockSize, float *h_out, int postprocess) {
   unsigned long long n;
   Geom g;
   if (!geom_ok(geom, &n, &g)) { set_error("invalid geometry"); return -1; }
@@ -786,7 +840,7 @@ int szp_b200_topo_decompress_host(szp_b200_ctx *ctx, const unsigned char *h_topo
   // block offsets of the topology stream from its bytes (the reference's walk)
   std::vector<unsigned long long> offs;
   unsigned long long hdr = 0, plen = 0;
-  if (!walk_stream(h_topo, n, B, true, offs, hdr, plen) || hdr + plen > topo_bytes) {
+  if (!walk_stream(h_topo, n, B, true, offs, hdr, plen, topo_bytes) || hdr + plen > topo_bytes) {
     set_error("malformed topology stream");
     return -1;
   }
@@ -826,7 +880,7 @@ int szp_b200_topo_decompress_host(szp_b200_ctx *ctx, const unsigned char *h_topo
     std::vector<unsigned long long> soffs;
     unsigned long long shdr = 0, splen = 0;
     if (E > 0) {
-      if (!walk_stream(h_sort, E, B, false, soffs, shdr, splen) || shdr + splen > sort_bytes) {
+      if (!walk_stream(h_sort, E, B, false, soffs, shdr, splen, sort_bytes) || shdr + splen > sort_bytes) {
         set_error("malformed sort-position stream");
         return -1;
       }
@@ -847,6 +901,42 @@ int szp_b200_topo_decompress_host(szp_b200_ctx *ctx, const unsigned char *h_topo
       cuda_fail(cudaStreamSynchronize(s), "sync"))
     return -1;
   return 0;
+}
+
+int szp_b200_topo_decompress_host(szp_b200_ctx *ctx, const unsigned char *h_topo, size_t topo_bytes,
+                                  const unsigned char *h_sort, size_t sort_bytes, szp_b200_geom geom,
+                                  float absErrBound, int blockSize, float *h_out, int postprocess) {
+  clear_error();
+  if (!ctx || !h_topo || !h_out) { set_error("null argument"); return -1; }
+  if (!check_block_size(blockSize, "szp_b200_topo_decompress_host")) return -1;
+  unsigned long long n;
+  Geom g;
+  if (!geom_ok(geom, &n, &g)) { set_error("invalid geometry"); return -1; }
+  // A single-chunk stream (offset table [0]) is parsed on the device; anything
+  // the device parser rejects goes through the reference's host detection.
+  if (topo_bytes > 8 && rd64(h_topo) == 0) {
+    const size_t sbytes = (h_sort && sort_bytes > 8) ? sort_bytes : 0;
+    if (!ctx->io.reserve(a256(topo_bytes) + a256(sbytes + 16) + a256(n * 4) + 4096)) return -1;
+    unsigned char *d_topo = ctx->io.take<unsigned char>(topo_bytes);
+    unsigned char *d_sort = ctx->io.take<unsigned char>(sbytes + 16);
+    float *d_out = ctx->io.take<float>(n);
+    cudaStream_t s = ctx->stream;
+    if (cuda_fail(cudaMemcpyAsync(d_topo, h_topo, topo_bytes, cudaMemcpyHostToDevice, s), "H2D") ||
+        (sbytes && cuda_fail(cudaMemcpyAsync(d_sort, h_sort, sbytes, cudaMemcpyHostToDevice, s), "H2D")))
+      return -1;
+    bool parse_failed = false;
+    if (decompress_dev_impl(ctx, d_topo, topo_bytes, sbytes ? d_sort : nullptr, sbytes, nullptr, geom,
+                            absErrBound, blockSize, d_out, nullptr, postprocess, true, &parse_failed) == 0) {
+      if (cuda_fail(cudaMemcpyAsync(h_out, d_out, n * 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+          cuda_fail(cudaStreamSynchronize(s), "sync"))
+        return -1;
+      return 0;
+    }
+    if (!parse_failed) return -1;
+    clear_error();
+  }
+  return decompress_host_walk(ctx, h_topo, topo_bytes, h_sort, sort_bytes, geom, absErrBound, blockSize,
+                              h_out, postprocess);
 }
 
 }  // extern "C"

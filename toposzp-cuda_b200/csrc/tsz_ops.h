@@ -41,4 +41,16 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
                      unsigned long long n_sp, const Geom &g, float eb, int axis_stencil,
                      int *restored_out);
 
+// Block offsets of a single-chunk stream, parsed on the device (enqueued on
+// ctx->stream, no sync).  d_payload: the bytes after the 8-byte offset table,
+// buf_len of them.  Element count n, or read on the device from d_n when it is
+// not null.  ref_bound adds the reference's validation bound (8n+1024 with
+// tags, 4n+4 without) to the buffer bound.  Writes the first ceil(n/B)
+// payload offsets to d_offs and d_status[0] = payload length + 1 on success
+// (0 when the walk failed), d_status[1] = nonzero on a malformed block.
+size_t parse_scratch_bytes(unsigned long long buf_len, int B, bool tags);
+int parse_stream(szp_b200_ctx *ctx, Arena &A, const unsigned char *d_payload, unsigned long long buf_len,
+                 unsigned long long n, const unsigned long long *d_n, int B, bool tags, bool ref_bound,
+                 unsigned long long *d_offs, unsigned long long *d_status);
+
 }  // namespace tsz

@@ -296,6 +296,8 @@ class Context:
 
     def decompress(self, topo, topo_bytes, sort, sort_bytes, index, shape, eb: float,
                    block_size: int = 64, postprocess: int = 1, out=None, types=None):
+        """Fused decompression of device streams.  index: the block index from
+        compress(), or None to parse the block offsets on the device."""
         import torch
         n = int(np.prod(shape))
         if out is None:
@@ -303,7 +305,7 @@ class Context:
         rc = lib().szp_b200_topo_decompress_dev(
             self.ptr, C.c_void_p(topo.data_ptr()), topo_bytes,
             C.c_void_p(sort.data_ptr()) if sort is not None else None, sort_bytes,
-            C.c_void_p(index.data_ptr()), geom_of(shape), eb, block_size,
+            C.c_void_p(index.data_ptr()) if index is not None else None, geom_of(shape), eb, block_size,
             C.c_void_p(out.data_ptr()), C.c_void_p(types.data_ptr()) if types is not None else None,
             postprocess)
         if rc:
