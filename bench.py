@@ -373,13 +373,13 @@ def main():
     codec = max([k for k in alg if k in stages], key=lambda k: stages[k])
     achieved = alg[codec] / (stages[codec] * 1e-3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    prof = os.path.join(ROOT, "profiles", "traffic.txt")
     if os.path.exists(prof):
-        try:
-            with open(prof) as fh:
-                traffic = json.load(fh).get(codec)
-        except Exception:
-            traffic = None
+        with open(prof) as fh:
+            for ln in fh:
+                parts = ln.split("#")[0].split()
+                if len(parts) == 2 and parts[0] == codec and args.side == 512:
+                    traffic = float(parts[1])
     rt_bytes = 2.0 * (4.0 * n + s_topo + s_sort)
     roofline = {"bound": "hbm", "kernel": codec, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
