@@ -201,6 +201,53 @@ SZP_B200_API int szp_b200_topo_postprocess_dev(szp_b200_ctx *ctx, float *d_data,
                                   const int *d_types, const int *d_sp, size_t n_sp,
                                   szp_b200_geom geom, float absErrBound, int axis_stencil);
 
+/* ------------------------------------------------------------------ */
+/* Batched compression (no reference counterpart)                      */
+/* ------------------------------------------------------------------ */
+
+/* One field of a batch.  errBound is absolute, or relative to the field's
+ * value range when rel != 0 (bound = errBound * (max - min) in float, as the
+ * reference's szp_rel_to_abs_float).  Buffers are device memory sized with
+ * szp_b200_topo_bound / szp_b200_sort_bound. */
+typedef struct {
+    const float *d_data;
+    szp_b200_geom geom;
+    float errBound;
+    int rel;
+    unsigned char *d_topo;
+    size_t topo_cap;
+    unsigned char *d_sort;
+    size_t sort_cap;
+    szp_b200_sizes sizes;   /* out */
+    float abs_eb;           /* out: the absolute bound the field was coded with */
+} szp_b200_batch_field;
+
+/* A batch compressor on a stream (0: its own stream) for one blockSize
+ * (at most 256).  Each call compresses any number of fields of any shapes
+ * with one persistent launch per codec pass (a device tile work-queue over
+ * all fields), replayed from captured CUDA graphs; the streams are the same
+ * bytes as szp_b200_topo_compress_dev gives per field.  The encoders' CTA
+ * shape (threads per CTA, CTAs per SM) is autotuned on the first batch. */
+typedef struct szp_b200_batch szp_b200_batch;
+SZP_B200_API szp_b200_batch *szp_b200_batch_create(void *cuda_stream, int blockSize);
+SZP_B200_API void szp_b200_batch_destroy(szp_b200_batch *b);
+
+/* use_graphs: replay captured CUDA graphs (1, default) or launch directly (0).
+ * autotune: 0 keep the current shapes, 1 tune once (default), 2 tune again. */
+SZP_B200_API int szp_b200_batch_configure(szp_b200_batch *b, int use_graphs, int autotune);
+
+/* Compresses count fields; fills each field's sizes and abs_eb.  Synchronous.
+ * Returns 0 on success. */
+SZP_B200_API int szp_b200_batch_compress(szp_b200_batch *b, szp_b200_batch_field *fields, int count);
+
+/* Chosen shapes: shape[0..3] = topology encoder threads per CTA, CTAs per SM,
+ * sort-position encoder threads per CTA, CTAs per SM; ms[] = the autotuner's
+ * timings of the topology-encoder candidates.  Returns 1 once tuned. */
+SZP_B200_API int szp_b200_batch_tuning(szp_b200_batch *b, int *shape, float *ms, int max);
+
+/* The batch's workspace (stage times, launch counter). */
+SZP_B200_API szp_b200_ctx *szp_b200_batch_ctx(szp_b200_batch *b);
+
 /* Topology stream of a device-resident field without any allocation (no
  * counterpart in the reference).  For callers that may not let a library
  * allocate device memory: code inside a framework that owns every device

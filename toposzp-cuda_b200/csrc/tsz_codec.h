@@ -45,6 +45,7 @@ struct DecArgs {
 };
 
 int enc_tile_blocks(int B);   // codec blocks per encoder tile (look-back granularity)
+int octet_group(int B);       // lanes per codec block in the octet kernels (B <= 256)
 int kmax_for(int B);
 int bpw_for(int kmax);
 int tile_blocks_for(int B);

@@ -120,8 +120,9 @@ __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, 
   return types;
 }
 
-// CTA-wide exclusive scan of one value per thread (kThreads threads);
+// CTA-wide exclusive scan of one value per thread (WARPS warps);
 // returns the exclusive prefix and writes the total to *total
+template <int WARPS = kWarps>
 __device__ __forceinline__ unsigned cta_excl_scan(unsigned v, unsigned *s_warp, unsigned *total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned inc = v;
@@ -134,7 +135,7 @@ __device__ __forceinline__ unsigned cta_excl_scan(unsigned v, unsigned *s_warp, 
   __syncthreads();
   unsigned wpre = 0, tot = 0;
 #pragma unroll
-  for (int w = 0; w < kWarps; w++) {
+  for (int w = 0; w < WARPS; w++) {
     const unsigned sw = s_warp[w];
     if (w < warp) wpre += sw;
     tot += sw;
@@ -143,36 +144,37 @@ __device__ __forceinline__ unsigned cta_excl_scan(unsigned v, unsigned *s_warp, 
   return wpre + inc - v;
 }
 
-template <int MODE, int G>
-__global__ void __launch_bounds__(kThreads, (MODE == kEncClassify ? 3 : 4))
-encode2_kernel(EncArgs a) {
-  constexpr int BPW = 32 / G;
-  constexpr int TB = kWarps * BPW;
-  extern __shared__ __align__(16) unsigned char smem_dyn[];
-  __shared__ uint32_t s_bytes[TB];
-  __shared__ unsigned s_w1[kWarps], s_w2[kWarps], s_w3[kWarps];
-  __shared__ long long s_tile;
-  __shared__ unsigned long long s_gbyte, s_gcnt;
-  __shared__ unsigned s_tile_bytes, s_tile_cps, s_tile_ext;
+// Shared state of one encoder CTA (WARPS warps, codec blocks of at most 8G
+// elements, 32/G blocks per warp).
+template <int G, int WARPS>
+struct EncShared {
+  static constexpr int TB = WARPS * (32 / G);
+  uint32_t bytes[TB];
+  unsigned w1[WARPS], w2[WARPS], w3[WARPS];
+  long long tile;
+  int field;
+  unsigned long long gbyte, gcnt;
+  unsigned tile_bytes, tile_cps, tile_ext;
+};
 
+// Encodes tile `tile` (TB codec blocks) of the field described by `a`: all
+// threads of the CTA call it; it ends with a CTA barrier.
+template <int MODE, int G, int WARPS>
+__device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long tile, unsigned char *img,
+                                             EncShared<G, WARPS> &sh) {
+  constexpr int BPW = 32 / G;
+  constexpr int TB = WARPS * BPW;
+  uint32_t *s_bytes = sh.bytes;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int gi = lane / G, l = lane % G;
   const bool tags = (MODE != kEncInts);
-  unsigned char *img = smem_dyn;
   uint32_t *imgw = reinterpret_cast<uint32_t *>(img);
-
   const long long n = (long long)a.n;
   const int B = a.B;
   const long long nblocks = (n + B - 1) / B;
   const long long ntiles = (nblocks + TB - 1) / TB;
-
-  while (true) {
-    if (threadIdx.x == 0) s_tile = (long long)atomicAdd(a.tile_ctr, 1u);
-    __syncthreads();
-    const long long tile = s_tile;
-    if (tile >= ntiles) break;
-
+  {
     const int bi = warp * BPW + gi;
     const long long blk = tile * TB + bi;
     const long long base = blk * B;
@@ -251,19 +253,19 @@ encode2_kernel(EncArgs a) {
     // ---- phase 2: tile scans (block bytes; per-thread CP / extremum counts) ----
     unsigned tbytes, tcps, text;
     const unsigned bv = (threadIdx.x < TB) ? s_bytes[threadIdx.x] : 0u;
-    const unsigned boff = cta_excl_scan(bv, s_w1, &tbytes);
-    const unsigned cpo = cta_excl_scan((unsigned)__popc(cpm), s_w2, &tcps);
-    const unsigned exo = cta_excl_scan((unsigned)__popc(exm), s_w3, &text);
+    const unsigned boff = cta_excl_scan<WARPS>(bv, sh.w1, &tbytes);
+    const unsigned cpo = cta_excl_scan<WARPS>((unsigned)__popc(cpm), sh.w2, &tcps);
+    const unsigned exo = cta_excl_scan<WARPS>((unsigned)__popc(exm), sh.w3, &text);
     __syncthreads();
     if (threadIdx.x < TB) s_bytes[threadIdx.x] = boff;
     if (threadIdx.x == 0) {
-      s_tile_bytes = tbytes;
-      s_tile_cps = tcps;
-      s_tile_ext = text;
+      sh.tile_bytes = tbytes;
+      sh.tile_cps = tcps;
+      sh.tile_ext = text;
       publish_aggregate(a.desc, tile, tbytes, ((unsigned long long)tcps << 32) | text);
     }
     __syncthreads();
-    const unsigned tile_bytes = s_tile_bytes;
+    const unsigned tile_bytes = sh.tile_bytes;
 
     // ---- phase 3: pack the octet into the tile image ----
     if (a.out != nullptr && nv > 0) {
@@ -341,20 +343,20 @@ encode2_kernel(EncArgs a) {
 
     // ---- phase 4: look-back (whole CTA) ----
     {
-      const Prefix pf = lookback_cta(a.desc, tile, tile_bytes,
-                                     ((unsigned long long)s_tile_cps << 32) | s_tile_ext, a.err);
+      const Prefix pf = lookback_cta<WARPS>(a.desc, tile, tile_bytes,
+                                            ((unsigned long long)sh.tile_cps << 32) | sh.tile_ext, a.err);
       if (threadIdx.x == 0) {
-        s_gbyte = pf.bytes;
-        s_gcnt = pf.cnt;
+        sh.gbyte = pf.bytes;
+        sh.gcnt = pf.cnt;
         if (tile == ntiles - 1 && a.total) {
           a.total[0] = pf.bytes + tile_bytes;
-          a.total[1] = (pf.cnt >> 32) + s_tile_cps;
-          a.total[2] = (pf.cnt & 0xffffffffull) + s_tile_ext;
+          a.total[1] = (pf.cnt >> 32) + sh.tile_cps;
+          a.total[2] = (pf.cnt & 0xffffffffull) + sh.tile_ext;
         }
       }
     }
     __syncthreads();
-    const unsigned long long G0 = s_gbyte;
+    const unsigned long long G0 = sh.gbyte;
     const bool fits = a.out != nullptr && (G0 + tile_bytes) <= a.out_cap;
     if (a.out != nullptr && !fits && threadIdx.x == 0) atomicExch(a.err, kErrOutputOverflow);
     if (a.blk_off && threadIdx.x < TB) {
@@ -372,7 +374,7 @@ encode2_kernel(EncArgs a) {
       const unsigned sh = 8u * (head & 3u);
       const unsigned w0 = head >> 2;
       uint4 *dq = reinterpret_cast<uint4 *>(dst + head);
-      for (unsigned qd = threadIdx.x; qd < nq; qd += kThreads) {
+      for (unsigned qd = threadIdx.x; qd < nq; qd += WARPS * 32) {
         const unsigned wi = w0 + 4u * qd;
         uint4 v;
         if (sh) {
@@ -391,8 +393,8 @@ encode2_kernel(EncArgs a) {
 
     // ---- phase 6: critical points in raster order (thread order == raster order) ----
     if (MODE == kEncClassify && a.cp_mode != kCpNone && cpm) {
-      unsigned long long ci = (s_gcnt >> 32) + cpo;
-      unsigned long long ei = (s_gcnt & 0xffffffffull) + exo;
+      unsigned long long ci = (sh.gcnt >> 32) + cpo;
+      unsigned long long ei = (sh.gcnt & 0xffffffffull) + exo;
 #pragma unroll
       for (int t = 0; t < 8; t++) {
         if (!(cpm & (1u << t))) continue;
@@ -424,6 +426,65 @@ encode2_kernel(EncArgs a) {
       }
     }
     __syncthreads();
+  }
+}
+
+// One field: persistent CTAs claim tiles from a.tile_ctr in order.
+template <int MODE, int G>
+__global__ void __launch_bounds__(kThreads, (MODE == kEncClassify ? 3 : 4))
+encode2_kernel(EncArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  __shared__ EncShared<G, kWarps> sh;
+  const long long nblocks = ((long long)a.n + a.B - 1) / a.B;
+  const long long ntiles = (nblocks + EncShared<G, kWarps>::TB - 1) / EncShared<G, kWarps>::TB;
+  while (true) {
+    if (threadIdx.x == 0) sh.tile = (long long)atomicAdd(a.tile_ctr, 1u);
+    __syncthreads();
+    const long long tile = sh.tile;
+    if (tile >= ntiles) break;
+    encode2_tile<MODE, G, kWarps>(a, tile, smem_dyn, sh);
+  }
+}
+
+// Many fields in one persistent launch: a device tile work-queue.  Tile t of
+// the queue is tile t - tile_start[f] of field f (tile_start[f] <= t <
+// tile_start[f+1]); a field's tiles leave the queue in order, so its
+// look-back always waits on tiles already held by running CTAs.
+template <int MODE, int G, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, (MODE == kEncClassify ? 24 : 32) / WARPS)
+encode2_batch_kernel(const EncArgs *__restrict__ fields, const unsigned long long *__restrict__ tile_start,
+                     const unsigned *__restrict__ nfields_dev, unsigned *queue) {
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  __shared__ EncShared<G, WARPS> sh;
+  __shared__ EncArgs s_a;
+  const int nf = (int)*nfields_dev;
+  const unsigned long long total = tile_start[nf];
+  int have = -1;
+  while (true) {
+    if (threadIdx.x == 0) {
+      const unsigned long long t = atomicAdd(queue, 1u);
+      if (t >= total) {
+        sh.tile = -1;
+      } else {
+        int lo = 0, hi = nf - 1;   // last field with tile_start <= t
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (tile_start[mid] <= t) lo = mid; else hi = mid - 1;
+        }
+        sh.field = lo;
+        sh.tile = (long long)(t - tile_start[lo]);
+      }
+    }
+    __syncthreads();
+    if (sh.tile < 0) break;
+    if (sh.field != have) {
+      have = sh.field;
+      const unsigned long long *src = reinterpret_cast<const unsigned long long *>(fields + have);
+      unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_a);
+      for (int w = threadIdx.x; w < (int)(sizeof(EncArgs) / 8); w += WARPS * 32) dst[w] = src[w];
+      __syncthreads();
+    }
+    encode2_tile<MODE, G, WARPS>(s_a, sh.tile, smem_dyn, sh);
   }
 }
 

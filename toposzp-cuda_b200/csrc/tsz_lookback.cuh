@@ -103,14 +103,15 @@ __device__ inline Prefix lookback(TileDesc *desc, long long t, unsigned long lon
 
 namespace tsz {
 
-// CTA-wide look-back: all kThreads threads of the CTA call it after the
-// tile's aggregate has been published.  Each round inspects kThreads
-// predecessors at once, so a walk back over P in-flight tiles takes about
-// P / kThreads rounds instead of P / 32.
+// CTA-wide look-back: all WARPS * 32 threads of the CTA call it after the
+// tile's aggregate has been published.  Each round inspects one predecessor
+// per thread, so a walk back over P in-flight tiles takes about P / (WARPS *
+// 32) rounds instead of P / 32.
+template <int WARPS = kWarps>
 __device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long long agg_bytes,
                                       unsigned long long agg_cnt, int *err) {
-  __shared__ unsigned s_first[kWarps];
-  __shared__ unsigned long long s_b[kWarps], s_c[kWarps];
+  __shared__ unsigned s_first[WARPS];
+  __shared__ unsigned long long s_b[WARPS], s_c[WARPS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   Prefix ex{0ull, 0ull};
   if (t == 0) return ex;
@@ -136,7 +137,7 @@ __device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long
     __syncthreads();
     unsigned first = 0xffffffffu;
 #pragma unroll
-    for (int w = 0; w < kWarps; w++) first = min(first, s_first[w]);
+    for (int w = 0; w < WARPS; w++) first = min(first, s_first[w]);
     unsigned long long b = 0, c = 0;
     if ((unsigned)threadIdx.x <= first && idx >= 0 && (st >> kStatShift) != 0ull) {
       b = st & kByteMask;
@@ -150,10 +151,10 @@ __device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long
     if (lane == 0) { s_b[warp] = b; s_c[warp] = c; }
     __syncthreads();
 #pragma unroll
-    for (int w = 0; w < kWarps; w++) { ex.bytes += s_b[w]; ex.cnt += s_c[w]; }
+    for (int w = 0; w < WARPS; w++) { ex.bytes += s_b[w]; ex.cnt += s_c[w]; }
     __syncthreads();
     if (first != 0xffffffffu) break;
-    base -= kThreads;
+    base -= WARPS * 32;
   }
   if (timed_out) atomicExch(err, kErrLookbackTimeout);
   if (threadIdx.x == 0) {

@@ -32,6 +32,12 @@ int postprocess(szp_b200_ctx *ctx, float *d_data, const float *d_orig,
                 int *restored_out);
 
 size_t rank_scratch_bytes(unsigned long long K, int sm_count);
+
+// Ranks of F segments in one pass (h_seg_K: records per segment, host);
+// bins disjoint across segments.
+int rank_positions_seg(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
+                       const unsigned long long *h_seg_K, int F, int *d_sp);
+size_t rank_scratch_bytes_seg(unsigned long long K, int F, int sm_count);
 size_t post_scratch_bytes(unsigned long long n);
 int compact_extrema(szp_b200_ctx *ctx, const int *d_cps, int stride, unsigned long long K, int *d_sp,
                     unsigned long long *E_out);

@@ -31,21 +31,30 @@ struct RankRec {
   int bin;
 };
 
+// A chunk of records that belongs to one segment (one field of a batch):
+// records [k0, k1) use buckets bbase .. bbase + NB - 1.
+struct SegChunk {
+  unsigned long long k0, k1;
+  unsigned long long bbase;
+};
+
 __device__ __forceinline__ int rec_bin(const uint2 &p, const int *bins, unsigned long long k,
                                        float eb, double inv) {
   return bins ? bins[k] : quant_bin(code_float(p.x), eb, inv);
 }
 
 // ---- 1a. per-CTA bucket histogram over a contiguous chunk -----------------
+// (seg != nullptr: CTA c takes chunk seg[c] instead of the c-th uniform chunk)
 __global__ void bucket_hist_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
                                    unsigned long long K, float eb, double inv, int logNB,
-                                   unsigned long long chunk, unsigned *__restrict__ M) {
+                                   unsigned long long chunk, unsigned *__restrict__ M,
+                                   const SegChunk *__restrict__ seg = nullptr) {
   extern __shared__ unsigned sh[];
   const int NB = 1 << logNB;
   for (int b = threadIdx.x; b < NB; b += blockDim.x) sh[b] = 0;
   __syncthreads();
-  const unsigned long long c0 = blockIdx.x * chunk;
-  const unsigned long long c1 = (c0 + chunk < K) ? c0 + chunk : K;
+  const unsigned long long c0 = seg ? seg[blockIdx.x].k0 : blockIdx.x * chunk;
+  const unsigned long long c1 = seg ? seg[blockIdx.x].k1 : ((c0 + chunk < K) ? c0 + chunk : K);
   for (unsigned long long k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
     const int bin = rec_bin(pairs[k], bins, k, eb, inv);
     atomicAdd(&sh[(unsigned)bin & (unsigned)(NB - 1)], 1u);
@@ -66,6 +75,22 @@ __global__ void bucket_colscan_kernel(unsigned *__restrict__ M, int G, int NB,
     run += v;
   }
   tot[b] = run;
+}
+
+// segmented column scan: bucket b of segment f scans the rows (chunks)
+// crow[f] .. crow[f+1]-1; its totals go to tot[f * NB + b]
+__global__ void bucket_colscan_seg_kernel(unsigned *__restrict__ M, const unsigned *__restrict__ crow, int F,
+                                          int NB, unsigned *__restrict__ tot) {
+  const long long gb = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gb >= (long long)F * NB) return;
+  const int f = (int)(gb / NB), b = (int)(gb % NB);
+  unsigned run = 0;
+  for (unsigned g = crow[f]; g < crow[f + 1]; g++) {
+    const unsigned v = M[(size_t)g * NB + b];
+    M[(size_t)g * NB + b] = run;
+    run += v;
+  }
+  tot[gb] = run;
 }
 
 // ---- 1c. exclusive scan of bucket totals (one CTA) -------------------------
@@ -102,7 +127,8 @@ __global__ void __launch_bounds__(kScatterThreads)
 bucket_scatter_sorted_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
                              unsigned long long K, float eb, double inv, int logNB,
                              unsigned long long chunk, const unsigned *__restrict__ M,
-                             const unsigned long long *__restrict__ start, RankRec *__restrict__ recs) {
+                             const unsigned long long *__restrict__ start_all, RankRec *__restrict__ recs,
+                             const SegChunk *__restrict__ seg = nullptr) {
   extern __shared__ unsigned char smx[];
   const int NB = 1 << logNB;
   unsigned *run = reinterpret_cast<unsigned *>(smx);          // records of this CTA already written per bucket
@@ -112,8 +138,9 @@ bucket_scatter_sorted_kernel(const uint2 *__restrict__ pairs, const int *__restr
   unsigned short *sb = reinterpret_cast<unsigned short *>(stage + kSub);  // bucket of each staged record
   __shared__ unsigned s_part[kScatterThreads / 32];
   for (int b = threadIdx.x; b < NB; b += blockDim.x) run[b] = M[(size_t)blockIdx.x * NB + b];
-  const unsigned long long c0 = blockIdx.x * chunk;
-  const unsigned long long c1 = (c0 + chunk < K) ? c0 + chunk : K;
+  const unsigned long long c0 = seg ? seg[blockIdx.x].k0 : blockIdx.x * chunk;
+  const unsigned long long c1 = seg ? seg[blockIdx.x].k1 : ((c0 + chunk < K) ? c0 + chunk : K);
+  const unsigned long long *start = start_all + (seg ? seg[blockIdx.x].bbase : 0ull);
   for (unsigned long long sub = c0; sub < c1; sub += kSub) {
     const int cnt = (int)((c1 - sub) < (unsigned long long)kSub ? (c1 - sub) : kSub);
     for (int b = threadIdx.x; b < NB; b += blockDim.x) hist[b] = 0;
@@ -309,6 +336,91 @@ bucket_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *_
   }
 }
 
+// ---- 2b. buckets the bitmap cannot hold, up to kSortCap records: sorted ----
+// in shared memory by (bin, code) (bitonic), then ranked by a segmented scan
+// (a new bin restarts at 0, every new distinct code adds 1).  Larger buckets
+// go on to the device-wide fallback.
+constexpr int kSortCap = 8192;
+constexpr int kSortThreads = 256;
+
+__global__ void __launch_bounds__(kSortThreads)
+bucket_sort_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *__restrict__ start,
+                        const unsigned *__restrict__ fb_list, const unsigned *__restrict__ fb_count,
+                        int *__restrict__ out, unsigned *__restrict__ fb2_list, unsigned *__restrict__ fb2_count) {
+  extern __shared__ unsigned long long sk[];
+  unsigned *sd = reinterpret_cast<unsigned *>(sk + kSortCap);
+  __shared__ unsigned s_flag[kSortThreads];
+  __shared__ unsigned s_val[kSortThreads];
+  if (blockIdx.x >= *fb_count) return;
+  const unsigned b = fb_list[blockIdx.x];
+  const unsigned long long r0 = start[b], r1 = start[b + 1];
+  const unsigned cnt = (unsigned)(r1 - r0);
+  if (r1 - r0 > (unsigned long long)kSortCap) {
+    if (threadIdx.x == 0) fb2_list[atomicAdd(fb2_count, 1u)] = b;
+    return;
+  }
+  unsigned P = 1;
+  while (P < cnt) P <<= 1;
+  for (unsigned i = threadIdx.x; i < P; i += blockDim.x) {
+    if (i < cnt) {
+      const RankRec r = recs[r0 + i];
+      sk[i] = ((unsigned long long)((unsigned)r.bin ^ 0x80000000u) << 32) | r.code;
+      sd[i] = r.dest;
+    } else {
+      sk[i] = ~0ull;
+      sd[i] = kNoExtremum;
+    }
+  }
+  __syncthreads();
+  for (unsigned k = 2; k <= P; k <<= 1) {
+    for (unsigned j = k >> 1; j > 0; j >>= 1) {
+      for (unsigned i = threadIdx.x; i < P; i += blockDim.x) {
+        const unsigned ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = sk[i], c = sk[ixj];
+          if ((a > c) == ((i & k) == 0)) {
+            sk[i] = c;
+            sk[ixj] = a;
+            const unsigned t = sd[i];
+            sd[i] = sd[ixj];
+            sd[ixj] = t;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // each thread owns a contiguous run of the sorted records
+  const unsigned per = (cnt + blockDim.x - 1) / blockDim.x;
+  const unsigned i0 = threadIdx.x * per, i1 = min(i0 + per, cnt);
+  unsigned flag = 0, val = 0;
+  for (unsigned i = i0; i < i1; i++) {
+    const bool st = (i == 0) || (sk[i] >> 32) != (sk[i - 1] >> 32);
+    if (st) { flag = 1; val = 0; }
+    else if ((unsigned)sk[i] != (unsigned)sk[i - 1]) val++;
+  }
+  s_flag[threadIdx.x] = flag;
+  s_val[threadIdx.x] = val;
+  __syncthreads();
+  // inclusive segmented scan over threads: (f1, v1) then (f2, v2) -> (f1|f2, f2 ? v2 : v1 + v2)
+  for (unsigned o = 1; o < blockDim.x; o <<= 1) {
+    unsigned pf = 0, pv = 0;
+    if (threadIdx.x >= o) { pf = s_flag[threadIdx.x - o]; pv = s_val[threadIdx.x - o]; }
+    __syncthreads();
+    if (threadIdx.x >= o && !s_flag[threadIdx.x]) { s_val[threadIdx.x] += pv; s_flag[threadIdx.x] = pf; }
+    __syncthreads();
+  }
+  unsigned run = threadIdx.x ? s_val[threadIdx.x - 1] : 0u;
+  for (unsigned i = i0; i < i1; i++) {
+    const bool st = (i == 0) || (sk[i] >> 32) != (sk[i - 1] >> 32);
+    if (st) run = 0;
+    else if ((unsigned)sk[i] != (unsigned)sk[i - 1]) run++;
+    if (sd[i] != kNoExtremum) out[sd[i]] = (int)run;
+  }
+}
+
+static size_t sort_rank_smem() { return (size_t)kSortCap * 12; }
+
 // ---- 3. fallback: device-wide LSD radix sort on (bin, code) ---------------
 // gather the records of the failed buckets into a contiguous list
 __global__ void fb_gather_count_kernel(const unsigned *__restrict__ fb_list, unsigned nfb,
@@ -457,6 +569,9 @@ __global__ void fb_rank_kernel(const unsigned long long *__restrict__ key,
   }
 }
 
+static int rank_fallback(szp_b200_ctx *ctx, RankRec *recs, const unsigned long long *start,
+                         const unsigned *fb_list, unsigned nfb, int *d_sp);
+
 int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
                    unsigned long long K, unsigned long long E, float eb, int *d_sp) {
   if (K == 0) return 0;
@@ -495,15 +610,28 @@ int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
   }
   if (cuda_fail(cudaMemsetAsync(fb_cnt, 0, 16, s), "memset")) return -1;
   bucket_rank_kernel<<<NB, kRankThreads, 0, s>>>(recs, start, logNB, d_sp, fb_list, fb_cnt);
-  ctx->launches += 5;
+  unsigned *fb2_list = A.take<unsigned>(NB);
+  if (!fb2_list) { set_error("scratch arena too small for the rank stage"); return -1; }
+  cudaFuncSetAttribute(bucket_sort_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_rank_smem());
+  bucket_sort_rank_kernel<<<NB, kSortThreads, sort_rank_smem(), s>>>(recs, start, fb_list, fb_cnt, d_sp, fb2_list,
+                                                                     fb_cnt + 1);
+  ctx->launches += 6;
   if (cuda_fail(cudaGetLastError(), "rank kernels")) return -1;
   unsigned nfb = 0;
-  if (cuda_fail(cudaMemcpyAsync(&nfb, fb_cnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+  if (cuda_fail(cudaMemcpyAsync(&nfb, fb_cnt + 1, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
       cuda_fail(cudaStreamSynchronize(s), "rank"))
     return -1;
   if (nfb == 0) return 0;
+  (void)E;
+  return rank_fallback(ctx, recs, start, fb2_list, nfb, d_sp);
+}
 
-  // ---- fallback ----
+// Buckets that did not fit the bitmap rank: their records are gathered and
+// ranked after a device-wide LSD radix sort on (bin, code).
+static int rank_fallback(szp_b200_ctx *ctx, RankRec *recs, const unsigned long long *start,
+                         const unsigned *fb_list, unsigned nfb, int *d_sp) {
+  cudaStream_t s = ctx->stream;
+  Arena &A = ctx->scratch;
   unsigned long long *fb_len = A.take<unsigned long long>(nfb + 1);
   if (!fb_len) { set_error("scratch arena too small for the rank fallback"); return -1; }
   fb_gather_count_kernel<<<(nfb + 255) / 256, 256, 0, s>>>(fb_list, nfb, start, fb_len);
@@ -537,8 +665,88 @@ int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
   if (cuda_fail(cudaGetLastError(), "fallback kernels") ||
       cuda_fail(cudaStreamSynchronize(s), "fallback"))
     return -1;
-  (void)E;
   return 0;
+}
+
+// Ranks of many segments (fields of a batch) in one pass: every segment gets
+// its own NB buckets and chunks never straddle segments, so records of
+// different segments never share a bucket.  bins must be disjoint across
+// segments (the fallback sorts all failing buckets together by bin).
+int rank_positions_seg(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
+                       const unsigned long long *h_seg_K, int F, int *d_sp) {
+  unsigned long long K = 0;
+  for (int f = 0; f < F; f++) K += h_seg_K[f];
+  if (K == 0) return 0;
+  cudaStream_t s = ctx->stream;
+  const int logNB = 9, NB = 1 << logNB;
+  unsigned long long chunk = std::max<unsigned long long>(4096, (K + 2 * ctx->sm_count - 1) / (2 * ctx->sm_count));
+  std::vector<SegChunk> chunks;
+  std::vector<unsigned> crow(F + 1);
+  unsigned long long k = 0;
+  for (int f = 0; f < F; f++) {
+    crow[f] = (unsigned)chunks.size();
+    const unsigned long long k1 = k + h_seg_K[f];
+    for (unsigned long long c = k; c < k1; c += chunk)
+      chunks.push_back({c, std::min(c + chunk, k1), (unsigned long long)f * NB});
+    k = k1;
+  }
+  crow[F] = (unsigned)chunks.size();
+  const unsigned C = (unsigned)chunks.size();
+  const unsigned long long nbk = (unsigned long long)F * NB;
+  Arena &A = ctx->scratch;
+  SegChunk *d_chunks = A.take<SegChunk>(C);
+  unsigned *d_crow = A.take<unsigned>(F + 1);
+  unsigned *M = A.take<unsigned>((size_t)C * NB);
+  unsigned *tot = A.take<unsigned>(nbk);
+  unsigned long long *start = A.take<unsigned long long>(nbk + 1);
+  RankRec *recs = A.take<RankRec>(K);
+  unsigned *fb_list = A.take<unsigned>(nbk);
+  unsigned *fb_cnt = A.take<unsigned>(4);
+  if (!d_chunks || !d_crow || !M || !tot || !start || !recs || !fb_list || !fb_cnt) {
+    set_error("scratch arena too small for the batched rank stage");
+    return -1;
+  }
+  if (cuda_fail(cudaMemcpyAsync(d_chunks, chunks.data(), C * sizeof(SegChunk), cudaMemcpyHostToDevice, s),
+                "H2D chunks") ||
+      cuda_fail(cudaMemcpyAsync(d_crow, crow.data(), (F + 1) * sizeof(unsigned), cudaMemcpyHostToDevice, s),
+                "H2D chunk rows"))
+    return -1;
+  const size_t hsm = (size_t)NB * 4;
+  cudaFuncSetAttribute(bucket_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm);
+  bucket_hist_kernel<<<C, 512, hsm, s>>>(d_pairs, d_bins, K, 1.0f, 1.0, logNB, chunk, M, d_chunks);
+  bucket_colscan_seg_kernel<<<(unsigned)((nbk + 255) / 256), 256, 0, s>>>(M, d_crow, F, NB, tot);
+  bucket_start_kernel<<<1, 1024, 0, s>>>(tot, (int)nbk, start);
+  {
+    const size_t ssm = (size_t)3 * NB * 4 + (size_t)kSub * sizeof(RankRec) + (size_t)kSub * 2 + 64;
+    cudaFuncSetAttribute(bucket_scatter_sorted_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm);
+    bucket_scatter_sorted_kernel<<<C, kScatterThreads, ssm, s>>>(d_pairs, d_bins, K, 1.0f, 1.0, logNB, chunk, M,
+                                                                 start, recs, d_chunks);
+  }
+  if (cuda_fail(cudaMemsetAsync(fb_cnt, 0, 16, s), "memset")) return -1;
+  bucket_rank_kernel<<<(unsigned)nbk, kRankThreads, 0, s>>>(recs, start, logNB, d_sp, fb_list, fb_cnt);
+  unsigned *fb2_list = A.take<unsigned>(nbk);
+  if (!fb2_list) { set_error("scratch arena too small for the batched rank stage"); return -1; }
+  cudaFuncSetAttribute(bucket_sort_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_rank_smem());
+  bucket_sort_rank_kernel<<<(unsigned)nbk, kSortThreads, sort_rank_smem(), s>>>(recs, start, fb_list, fb_cnt, d_sp,
+                                                                                fb2_list, fb_cnt + 1);
+  ctx->launches += 6;
+  if (cuda_fail(cudaGetLastError(), "batched rank kernels")) return -1;
+  unsigned nfb = 0;
+  if (cuda_fail(cudaMemcpyAsync(&nfb, fb_cnt + 1, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaStreamSynchronize(s), "rank"))
+    return -1;
+  if (nfb == 0) return 0;
+  return rank_fallback(ctx, recs, start, fb2_list, nfb, d_sp);
+}
+
+size_t rank_scratch_bytes_seg(unsigned long long K, int F, int sm_count) {
+  const size_t NB = 512;
+  const unsigned long long chunk = std::max<unsigned long long>(4096, (K + 2 * sm_count - 1) / (2 * sm_count));
+  const size_t C = (size_t)(K / chunk) + (size_t)F + 1;
+  const size_t nbk = (size_t)F * NB;
+  const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4);
+  return a256(C * sizeof(SegChunk)) + a256((F + 1) * 4) + a256(C * NB * 4) + a256(nbk * 4) +
+         a256((nbk + 1) * 8) + a256(K * sizeof(RankRec)) + a256(nbk * 4) * 2 + a256(16) + fb + a256(nbk * 8) + 8192;
 }
 
 size_t rank_scratch_bytes(unsigned long long K, int sm_count) {
@@ -549,7 +757,7 @@ size_t rank_scratch_bytes(unsigned long long K, int sm_count) {
   // fallback worst case: all K records (two key/value ping-pong buffers + histogram)
   const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4);
   return a256(G * NB * 4) + a256(NB * 4) + a256((NB + 1) * 8) + a256(K * sizeof(RankRec)) +
-         a256(NB * 4) * 2 + a256(16) + fb + 4096;
+         a256(NB * 4) * 3 + a256(16) + fb + 4096;
 }
 
 // ---------------------------------------------------------------------------

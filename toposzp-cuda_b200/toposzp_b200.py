@@ -49,6 +49,12 @@ EXPORTS = [
     "szp_b200_topo_compress_host",
     "szp_b200_topo_decompress_host",
     "szp_b200_topo_encode_noalloc",
+    "szp_b200_batch_create",
+    "szp_b200_batch_destroy",
+    "szp_b200_batch_configure",
+    "szp_b200_batch_compress",
+    "szp_b200_batch_tuning",
+    "szp_b200_batch_ctx",
 ]
 
 
@@ -63,6 +69,12 @@ class Geom(C.Structure):
 class Sizes(C.Structure):
     _fields_ = [("topo_bytes", C.c_size_t), ("sort_bytes", C.c_size_t),
                 ("cp_count", C.c_size_t), ("extrema_count", C.c_size_t)]
+
+
+class BatchField(C.Structure):
+    _fields_ = [("d_data", C.c_void_p), ("geom", Geom), ("errBound", C.c_float), ("rel", C.c_int),
+                ("d_topo", C.c_void_p), ("topo_cap", C.c_size_t), ("d_sort", C.c_void_p),
+                ("sort_cap", C.c_size_t), ("sizes", Sizes), ("abs_eb", C.c_float)]
 
 
 def build() -> str:
@@ -110,6 +122,12 @@ def lib():
             "szp_b200_topo_compress_host": (i, [vp, vp, Geom, f, i, vp, sz, vp, sz, C.POINTER(Sizes)]),
             "szp_b200_topo_decompress_host": (i, [vp, vp, sz, vp, sz, Geom, f, i, vp, i]),
             "szp_b200_topo_encode_noalloc": (i, [vp, Geom, f, i, vp, sz, C.POINTER(sz), vp]),
+            "szp_b200_batch_create": (vp, [vp, i]),
+            "szp_b200_batch_destroy": (None, [vp]),
+            "szp_b200_batch_configure": (i, [vp, i, i]),
+            "szp_b200_batch_compress": (i, [vp, C.POINTER(BatchField), i]),
+            "szp_b200_batch_tuning": (i, [vp, C.POINTER(C.c_int), C.POINTER(C.c_float), i]),
+            "szp_b200_batch_ctx": (vp, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -353,3 +371,78 @@ class Context:
         if rc:
             raise ToposzpError(last_error())
         return d_data
+
+
+class Batch:
+    """Batched compression of many device fields (one persistent launch per
+    codec pass, CUDA-graph replay, autotuned CTA shapes)."""
+
+    def __init__(self, block_size: int = 64, stream_handle: int = 0):
+        self.B = block_size
+        self.ptr = lib().szp_b200_batch_create(C.c_void_p(stream_handle) if stream_handle else None, block_size)
+        if not self.ptr:
+            raise ToposzpError(last_error())
+        self._bufs = []
+
+    def close(self):
+        if self.ptr:
+            lib().szp_b200_batch_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def configure(self, use_graphs: bool = True, autotune: int = 1):
+        if lib().szp_b200_batch_configure(self.ptr, int(use_graphs), int(autotune)):
+            raise ToposzpError(last_error())
+
+    def buffers(self, items):
+        """Device output buffers sized for items [(tensor, shape, err, rel)]."""
+        import torch
+        L = lib()
+        out = []
+        for t, shape, _, _ in items:
+            n = int(np.prod(shape))
+            out.append((torch.empty(L.szp_b200_topo_bound(n, self.B), dtype=torch.uint8, device=t.device),
+                        torch.empty(L.szp_b200_sort_bound(n, self.B), dtype=torch.uint8, device=t.device)))
+        return out
+
+    def compress(self, items, bufs=None):
+        """items: [(device float tensor, shape, err, rel)].  Returns
+        [(topo, sort, Sizes, abs_eb)] with topo / sort the device buffers."""
+        if bufs is None:
+            bufs = self.buffers(items)
+        arr = (BatchField * len(items))()
+        for k, ((t, shape, err, rel), (tb, sb)) in enumerate(zip(items, bufs)):
+            arr[k].d_data = t.data_ptr()
+            arr[k].geom = geom_of(shape)
+            arr[k].errBound = err
+            arr[k].rel = int(bool(rel))
+            arr[k].d_topo = tb.data_ptr()
+            arr[k].topo_cap = tb.numel()
+            arr[k].d_sort = sb.data_ptr()
+            arr[k].sort_cap = sb.numel()
+        if lib().szp_b200_batch_compress(self.ptr, arr, len(items)):
+            raise ToposzpError(last_error())
+        return [(tb, sb, arr[k].sizes, float(arr[k].abs_eb)) for k, (tb, sb) in enumerate(bufs)]
+
+    def tuning(self):
+        shape = (C.c_int * 4)()
+        ms = (C.c_float * 16)()
+        tuned = lib().szp_b200_batch_tuning(self.ptr, shape, ms, 16)
+        return {"tuned": bool(tuned), "topo_threads": shape[0], "topo_ctas_per_sm": shape[1],
+                "sort_threads": shape[2], "sort_ctas_per_sm": shape[3],
+                "topo_candidates_ms": [round(float(x), 4) for x in ms if x > 0]}
+
+    def stage_times(self):
+        c = lib().szp_b200_batch_ctx(self.ptr)
+        names = (C.c_char_p * 24)()
+        ms = (C.c_float * 24)()
+        k = lib().szp_b200_ctx_stage_times(c, names, ms, 24)
+        return [(names[i].decode(), float(ms[i])) for i in range(k)]
+
+    def launches(self) -> int:
+        return int(lib().szp_b200_ctx_launches(lib().szp_b200_batch_ctx(self.ptr)))
