@@ -313,6 +313,137 @@ def batch_leg(T, dev, steps, warmup, count=256):
 
 
 # ---------------------------------------------------------------------------
+# served leg: Poisson request stream with continuous batching vs plain calls
+# ---------------------------------------------------------------------------
+
+def serve_pool(count=32, seed=4):
+    """Fields of the request stream: sizes log-uniform over 16 KB - 256 MB of
+    fp32, 2D or 3D, Gaussian-bump generator; generated once and cached."""
+    import math
+    rng = np.random.default_rng(seed)
+    pool = []
+    for k in range(count):
+        nbytes = math.exp(rng.uniform(math.log(16e3), math.log(256e6)))
+        n = max(4096, int(nbytes / 4))
+        if rng.random() < 0.5:
+            a = int(round(math.sqrt(n) * math.exp(rng.uniform(-0.3, 0.3))))
+            dims = (max(3, a), max(3, n // max(3, a)))
+        else:
+            a = int(round(n ** (1 / 3)))
+            dims = (max(3, a), max(3, a), max(3, n // max(3, a) // max(3, a)))
+        nb = 20 if len(dims) == 2 else 40
+        side = min(dims)
+        data = synth._cached("serve_%d_%d" % (seed, k), dims,
+                             lambda dims=dims, nb=nb, side=side, k=k: synth.gaussian_bumps(
+                                 dims, nb, max(1.0, 0.03 * side), max(2.0, 0.25 * side), 1e-3, 1000 + k))
+        pool.append((dims, data))
+    return pool
+
+
+def serve_leg(T, dev, nreq=400, slots=4, rate=2000.0, seed=4):
+    """Served mode against back-to-back plain calls on the same requests.
+    Served: requests submitted at their Poisson arrival times to the server
+    (continuous batching, HBM budget 120 GiB); latency = completion - arrival.
+    Plain: the same requests one after another on one stream, each timed with
+    CUDA events; its latencies follow from the same arrivals through a FIFO
+    queue (start = max(arrival, previous completion))."""
+    import torch
+    rng = np.random.default_rng(seed)
+    pool = serve_pool(seed=seed)
+    L = T.lib()
+    d_pool = [torch.from_numpy(d.reshape(-1)).to(dev) for _, d in pool]
+    stream = torch.cuda.Stream(device=dev)
+    ctx = T.Context(stream.cuda_stream)
+    # streams of every pool field for the decompress requests (untimed setup)
+    pre = []
+    for (dims, _), d in zip(pool, d_pool):
+        eb = float(10 ** rng.uniform(-4, -2))
+        topo, sort, _, sz = ctx.compress(d, dims, eb, 64, index=False)
+        pre.append((topo, sz.topo_bytes, sort, sz.sort_bytes, eb))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
+    ops = rng.random(nreq) < 0.7
+    picks = rng.integers(0, len(pool), size=nreq)
+    ebs = 10 ** rng.uniform(-4, -2, size=nreq)
+    srv = T.Server(slots=slots, max_batch=64, block_size=64, hbm_budget=120 << 30)
+    spec = []
+    for i in range(nreq):
+        dims = pool[picks[i]][0]
+        n = int(np.prod(dims))
+        if ops[i]:
+            spec.append(("c", picks[i], float(ebs[i]),
+                         torch.empty(L.szp_b200_topo_bound(n, 64), dtype=torch.uint8, device=dev),
+                         torch.empty(L.szp_b200_sort_bound(n, 64), dtype=torch.uint8, device=dev)))
+        else:
+            spec.append(("d", picks[i], torch.empty(n, dtype=torch.float32, device=dev)))
+
+    def requests(sel):
+        arr = (T.Request * len(sel))()
+        for j, i in enumerate(sel):
+            sp = spec[i]
+            dims = pool[sp[1]][0]
+            if sp[0] == "c":
+                arr[j] = srv.compress_request(d_pool[sp[1]], dims, sp[2], False, sp[3], sp[4])
+            else:
+                topo, tn, sort, sn, eb = pre[sp[1]]
+                arr[j] = srv.decompress_request(topo, tn, sort if sn else None, sn, dims, eb, sp[2], 1)
+        return arr
+    # warm-up: autotuning and workspace growth in every slot
+    warm = list(range(min(nreq, 160)))
+    srv.run_trace(requests(warm))
+    srv.run_trace(requests(warm))
+    torch.cuda.synchronize()
+    arr = requests(list(range(nreq)))
+    st0 = srv.stats()
+    srv.run_trace(arr, arrivals.tolist())
+    st = srv.stats()
+    lat = np.array([r.t_done - r.t_arrival for r in arr]) * 1e3
+    span = max(r.t_done for r in arr) - min(r.t_arrival for r in arr)
+    nbytes = np.array([4.0 * np.prod(pool[sp[1]][0]) for sp in spec])
+    import ctypes as C
+    sizes = T.Sizes()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    svc = np.zeros(nreq)
+    for rep in range(2):
+        for i, sp in enumerate(spec):
+            dims = pool[sp[1]][0]
+            ev[0].record(stream)
+            if sp[0] == "c":
+                rc = L.szp_b200_topo_compress_dev(ctx.ptr, C.c_void_p(d_pool[sp[1]].data_ptr()), T.geom_of(dims),
+                                                  sp[2], 64, C.c_void_p(sp[3].data_ptr()),
+                                                  C.c_void_p(sp[4].data_ptr()), None, C.byref(sizes))
+            else:
+                topo, tn, sort, sn, eb = pre[sp[1]]
+                rc = L.szp_b200_topo_decompress_dev(ctx.ptr, C.c_void_p(topo.data_ptr()), tn,
+                                                    C.c_void_p(sort.data_ptr()) if sn else None, sn, None,
+                                                    T.geom_of(dims), eb, 64, C.c_void_p(sp[2].data_ptr()), None, 1)
+            if rc:
+                raise T.ToposzpError(T.last_error())
+            ev[1].record(stream)
+            ev[1].synchronize()
+            svc[i] = ev[0].elapsed_time(ev[1]) * 1e-3
+    t = 0.0
+    plat = np.zeros(nreq)
+    for i in range(nreq):
+        t = max(t, arrivals[i]) + svc[i]
+        plat[i] = (t - arrivals[i]) * 1e3
+    pspan = t - arrivals[0]
+    out = {"workload": "c5 served: %d requests, Poisson %.0f req/s (seed %d), 70%% compress / 30%% decompress "
+                       "(with post-processing), fields 16 KB-256 MB log-uniform (pool of %d 2D/3D bump fields), "
+                       "abs eb log-U[1e-4,1e-2], HBM budget 120 GiB, %d slots" % (nreq, rate, seed, len(pool), slots),
+           "served_gbs": float(nbytes.sum() / span / 1e9), "served_p50_ms": float(np.percentile(lat, 50)),
+           "served_p99_ms": float(np.percentile(lat, 99)),
+           "plain_gbs": float(nbytes.sum() / pspan / 1e9), "plain_p50_ms": float(np.percentile(plat, 50)),
+           "plain_p99_ms": float(np.percentile(plat, 99)),
+           "plain_busy_s": float(svc.sum()), "served_span_s": float(span),
+           "batches": st["batches"] - st0["batches"],
+           "batched_requests": st["batched_requests"] - st0["batched_requests"],
+           "max_concurrent": st["max_concurrent"], "max_inflight_gb": st["max_inflight_bytes"] / 1e9}
+    srv.close()
+    ctx.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # main
 # ---------------------------------------------------------------------------
 
@@ -327,6 +458,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-vs-plain leg")
     return ap.parse_args()
 
 
@@ -502,6 +634,10 @@ def main():
     if not args.no_batch:
         batched = batch_leg(T, dev, max(3, min(args.steps, 5)), args.warmup)
 
+    served = None
+    if not args.no_serve:
+        served = serve_leg(T, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = reference_leg(f, args.cpu_planes, os.cpu_count() or 1)
@@ -528,6 +664,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "batched": batched,
+            "served": served,
         }
         print(json.dumps(line))
     ctx.close()

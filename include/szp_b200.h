@@ -248,6 +248,73 @@ SZP_B200_API int szp_b200_batch_tuning(szp_b200_batch *b, int *shape, float *ms,
 /* The batch's workspace (stage times, launch counter). */
 SZP_B200_API szp_b200_ctx *szp_b200_batch_ctx(szp_b200_batch *b);
 
+/* ------------------------------------------------------------------ */
+/* Request server with continuous batching (no reference counterpart)  */
+/* ------------------------------------------------------------------ */
+
+#define SZP_B200_OP_COMPRESS 0
+#define SZP_B200_OP_DECOMPRESS 1
+
+typedef struct {
+    int slots;            /* concurrent workers: one stream + workspace + batch compressor each */
+    int max_batch;        /* compressions merged into one batched launch */
+    int blockSize;        /* blockSize of the compressions (at most 256) */
+    size_t hbm_budget;    /* estimated device bytes admitted at once (0: 120 GiB); one merged
+                             launch takes at most hbm_budget / slots */
+} szp_b200_server_config;
+
+/* One request; it must stay alive and untouched until done != 0.  All
+ * buffers are device memory owned by the caller.
+ *   compress:   d_data in; d_topo / d_sort out with topo_bytes / sort_bytes
+ *               their capacities; errBound absolute, or relative when rel
+ *   decompress: d_topo / d_sort in with topo_bytes / sort_bytes their stream
+ *               lengths (block offsets parsed on the device); d_out out;
+ *               errBound absolute; postprocess as szp_b200_topo_decompress_dev */
+typedef struct {
+    int op;
+    int blockSize;
+    szp_b200_geom geom;
+    float errBound;
+    int rel;
+    int postprocess;
+    const float *d_data;
+    float *d_out;
+    unsigned char *d_topo;
+    size_t topo_bytes;
+    unsigned char *d_sort;
+    size_t sort_bytes;
+    szp_b200_sizes sizes;     /* out (compress) */
+    float abs_eb;             /* out (compress) */
+    int status;               /* out: 0 ok, -1 failed (message), 1 pending */
+    int done;                 /* out: set when the request has finished */
+    double t_arrival;         /* server clock, seconds: arrival (set on submit when 0) */
+    double t_start;           /* out: taken by a worker */
+    double t_done;            /* out: finished */
+    char message[96];         /* out: error text */
+} szp_b200_request;
+
+typedef struct {
+    unsigned long long submitted, completed, failed;
+    unsigned long long batches, batched_requests;   /* batched compress launches, requests in them */
+    size_t max_inflight_bytes;                      /* peak admitted working set */
+    int max_concurrent;                             /* peak requests in flight */
+} szp_b200_server_stats_t;
+
+typedef struct szp_b200_server szp_b200_server;
+SZP_B200_API szp_b200_server *szp_b200_server_create(const szp_b200_server_config *cfg);
+SZP_B200_API void szp_b200_server_destroy(szp_b200_server *s);
+SZP_B200_API double szp_b200_server_now(szp_b200_server *s);
+SZP_B200_API int szp_b200_server_submit(szp_b200_server *s, szp_b200_request *r);
+/* 0 when r finished within timeout_s, 1 on timeout */
+SZP_B200_API int szp_b200_server_wait(szp_b200_server *s, szp_b200_request *r, double timeout_s);
+/* 0 when every submitted request finished within timeout_s, 1 on timeout */
+SZP_B200_API int szp_b200_server_drain(szp_b200_server *s, double timeout_s);
+/* Submits reqs[i] at arrival_s[i] seconds after the call (NULL: all at once),
+ * then drains. */
+SZP_B200_API int szp_b200_server_run_trace(szp_b200_server *s, szp_b200_request *reqs, int n,
+                                           const double *arrival_s, double timeout_s);
+SZP_B200_API int szp_b200_server_stats(szp_b200_server *s, szp_b200_server_stats_t *st);
+
 /* Topology stream of a device-resident field without any allocation (no
  * counterpart in the reference).  For callers that may not let a library
  * allocate device memory: code inside a framework that owns every device

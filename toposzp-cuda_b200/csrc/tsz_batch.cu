@@ -777,6 +777,15 @@ int szp_b200_batch_compress(szp_b200_batch *b, szp_b200_batch_field *fs, int cou
   if (b->cap_f != oldcap || b->cap_tiles != oldt || b->cap_pairs != oldp || b->cap_itiles != oldi) drop_graphs(b);
   szp_b200_ctx *ctx = b->ctx;
   cudaStream_t s = ctx->stream;
+  if (b->autotune == 1 && !b->tuned) {
+    // shapes already tuned on this device by another batch object
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    int found = 0;
+    for (int m = 0; m < 2; m++)
+      for (auto &kv : g_tune_cache)
+        if (kv.first == tune_key(ctx->device, B, m)) { b->tune[m] = kv.second; found++; }
+    if (found == 2) { b->tuned = true; drop_graphs(b); }
+  }
   const bool tune_now = b->autotune && !b->tuned;
   tl_begin(ctx);
   if (tune_now) {

@@ -55,7 +55,18 @@ EXPORTS = [
     "szp_b200_batch_compress",
     "szp_b200_batch_tuning",
     "szp_b200_batch_ctx",
+    "szp_b200_server_create",
+    "szp_b200_server_destroy",
+    "szp_b200_server_now",
+    "szp_b200_server_submit",
+    "szp_b200_server_wait",
+    "szp_b200_server_drain",
+    "szp_b200_server_run_trace",
+    "szp_b200_server_stats",
 ]
+
+OP_COMPRESS = 0
+OP_DECOMPRESS = 1
 
 
 class ToposzpError(RuntimeError):
@@ -69,6 +80,26 @@ class Geom(C.Structure):
 class Sizes(C.Structure):
     _fields_ = [("topo_bytes", C.c_size_t), ("sort_bytes", C.c_size_t),
                 ("cp_count", C.c_size_t), ("extrema_count", C.c_size_t)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("slots", C.c_int), ("max_batch", C.c_int), ("blockSize", C.c_int),
+                ("hbm_budget", C.c_size_t)]
+
+
+class Request(C.Structure):
+    _fields_ = [("op", C.c_int), ("blockSize", C.c_int), ("geom", Geom), ("errBound", C.c_float),
+                ("rel", C.c_int), ("postprocess", C.c_int), ("d_data", C.c_void_p), ("d_out", C.c_void_p),
+                ("d_topo", C.c_void_p), ("topo_bytes", C.c_size_t), ("d_sort", C.c_void_p),
+                ("sort_bytes", C.c_size_t), ("sizes", Sizes), ("abs_eb", C.c_float), ("status", C.c_int),
+                ("done", C.c_int), ("t_arrival", C.c_double), ("t_start", C.c_double),
+                ("t_done", C.c_double), ("message", C.c_char * 96)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_ulonglong), ("completed", C.c_ulonglong), ("failed", C.c_ulonglong),
+                ("batches", C.c_ulonglong), ("batched_requests", C.c_ulonglong),
+                ("max_inflight_bytes", C.c_size_t), ("max_concurrent", C.c_int)]
 
 
 class BatchField(C.Structure):
@@ -128,6 +159,14 @@ def lib():
             "szp_b200_batch_compress": (i, [vp, C.POINTER(BatchField), i]),
             "szp_b200_batch_tuning": (i, [vp, C.POINTER(C.c_int), C.POINTER(C.c_float), i]),
             "szp_b200_batch_ctx": (vp, [vp]),
+            "szp_b200_server_create": (vp, [C.POINTER(ServerConfig)]),
+            "szp_b200_server_destroy": (None, [vp]),
+            "szp_b200_server_now": (C.c_double, [vp]),
+            "szp_b200_server_submit": (i, [vp, C.POINTER(Request)]),
+            "szp_b200_server_wait": (i, [vp, C.POINTER(Request), C.c_double]),
+            "szp_b200_server_drain": (i, [vp, C.c_double]),
+            "szp_b200_server_run_trace": (i, [vp, C.POINTER(Request), i, C.POINTER(C.c_double), C.c_double]),
+            "szp_b200_server_stats": (i, [vp, C.POINTER(ServerStats)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -446,3 +485,64 @@ class Batch:
 
     def launches(self) -> int:
         return int(lib().szp_b200_ctx_launches(lib().szp_b200_batch_ctx(self.ptr)))
+
+
+class Server:
+    """Request server with continuous batching (compress / decompress of
+    device-resident fields, HBM admission budget, per-request timing)."""
+
+    def __init__(self, slots: int = 4, max_batch: int = 64, block_size: int = 64, hbm_budget: int = 0):
+        cfg = ServerConfig(slots, max_batch, block_size, hbm_budget)
+        self.B = block_size
+        self.ptr = lib().szp_b200_server_create(C.byref(cfg))
+        if not self.ptr:
+            raise ToposzpError(last_error())
+
+    def close(self):
+        if self.ptr:
+            lib().szp_b200_server_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compress_request(self, d_data, shape, err, rel, d_topo, d_sort) -> Request:
+        r = Request()
+        r.op, r.blockSize, r.geom = OP_COMPRESS, self.B, geom_of(shape)
+        r.errBound, r.rel = err, int(bool(rel))
+        r.d_data = d_data.data_ptr()
+        r.d_topo, r.topo_bytes = d_topo.data_ptr(), d_topo.numel()
+        r.d_sort, r.sort_bytes = d_sort.data_ptr(), d_sort.numel()
+        return r
+
+    def decompress_request(self, d_topo, topo_bytes, d_sort, sort_bytes, shape, abs_eb, d_out,
+                           postprocess: int = 1) -> Request:
+        r = Request()
+        r.op, r.blockSize, r.geom = OP_DECOMPRESS, self.B, geom_of(shape)
+        r.errBound, r.postprocess = abs_eb, postprocess
+        r.d_topo, r.topo_bytes = d_topo.data_ptr(), topo_bytes
+        r.d_sort, r.sort_bytes = (d_sort.data_ptr() if d_sort is not None else None), sort_bytes
+        r.d_out = d_out.data_ptr()
+        return r
+
+    def run_trace(self, reqs, arrivals=None, timeout: float = 600.0):
+        """Submits the Request array reqs (a ctypes array) at the given arrival
+        offsets in seconds (None: all at once) and waits for all of them."""
+        arr = (C.c_double * len(reqs))(*arrivals) if arrivals is not None else None
+        rc = lib().szp_b200_server_run_trace(self.ptr, reqs, len(reqs), arr, timeout)
+        if rc < 0:
+            raise ToposzpError(last_error())
+        if rc > 0:
+            raise ToposzpError("server trace timed out")
+        for r in reqs:
+            if r.status != 0:
+                raise ToposzpError(r.message.decode())
+        return reqs
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        lib().szp_b200_server_stats(self.ptr, C.byref(st))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
