@@ -469,23 +469,26 @@ def run_reference_arm(args):
         return 0
     f = synth.config3(args.side)
     threads = os.cpu_count() or 1
+    # each step is a bounded sample: about 25 s of CPU work over all steps at
+    # 256 planes per 10 s, never fewer than 16 planes
+    planes = int(min(args.cpu_planes, max(16, 640 // max(1, args.steps))))
     for _ in range(args.warmup):
-        reference_leg(f, max(4, args.cpu_planes // 4), threads)
+        reference_leg(f, 4, threads)
     vals, info = [], None
     for _ in range(args.steps):
-        info = reference_leg(f, args.cpu_planes, threads)
+        info = reference_leg(f, planes, threads)
         vals.append(info["value"])
     v = statistics.median(vals)
     info = dict(info, value=v)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 4.0 * args.cpu_planes * args.side * args.side / v / 1e6,
+        "ms_per_step": 4.0 * planes * args.side * args.side / v / 1e6,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded band-limited field)",
         "config": {"workload": "%s: %d^3 band-limited fp32 field, abs eb 1e-4, blockSize 64, "
                                "round trip with post-processing; CPU sample = first %d planes"
-                               % (f.name, args.side, args.cpu_planes),
+                               % (f.name, args.side, planes),
                    "threads": threads},
         "cpu_baseline": info,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
