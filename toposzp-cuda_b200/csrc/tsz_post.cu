@@ -76,6 +76,8 @@ struct PostArgs {
   unsigned *tile_ctr;
   int *err;
   unsigned *restored;
+  bool prev_in_S;               // this pass's candidates hold their pre-pass values in S
+                                // (the previous pass ran over the same list, unscattered)
 };
 
 __device__ __forceinline__ unsigned long long ld_rlx(const unsigned long long *p) {
@@ -231,6 +233,16 @@ __device__ float stencil3(const PostArgs &a, long long e, const C3 &c, int t, in
   return clampf(target, lo, hi);
 }
 
+// pre-pass value of the enforcement pass at e + (dx, dy, dz), for e itself and
+// later points: after an unscattered stencil pass a candidate's value is its
+// stencil result in S; every other point still holds its value in F
+__device__ __forceinline__ float pre_value(const PostArgs &a, long long e, const C3 &c, int dx, int dy, int dz) {
+  const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
+  if (a.prev_in_S && is_cand_known<kPassEnforce>(a, q, interior_off(a, c, dx, dy, dz)))
+    return __uint_as_float((unsigned)ld_rlx(&a.S[q]));
+  return a.F[q];
+}
+
 // enforcement (example/test_cuda_topology.cu:168-198, _3d.cu:131-167)
 template <int ND>
 __device__ float enforce(const PostArgs &a, long long e, const C3 &c, int t) {
@@ -238,18 +250,16 @@ __device__ float enforce(const PostArgs &a, long long e, const C3 &c, int t) {
   const float d = __fmul_rn(a.eb, 0.999f);
   const float hi = __fadd_rn(o, d), lo = __fsub_rn(o, d);
   const float soft = __fmul_rn(0.25f, a.eps);
-  const float cur = a.F[e];
+  const float cur = pre_value(a, e, c, 0, 0, 0);
   float m;
   if (ND == 2) {
-    const long long cols = a.g.d3;
-    const float n = valo<kPassEnforce>(a, e, c, 0, -1, 0), s = a.F[e + cols];
-    const float w = valo<kPassEnforce>(a, e, c, 0, 0, -1), ea = a.F[e + 1];
+    const float n = valo<kPassEnforce>(a, e, c, 0, -1, 0), s = pre_value(a, e, c, 0, 1, 0);
+    const float w = valo<kPassEnforce>(a, e, c, 0, 0, -1), ea = pre_value(a, e, c, 0, 0, 1);
     m = (t == 1) ? fmaxf(fmaxf(n, s), fmaxf(w, ea)) : fminf(fminf(n, s), fminf(w, ea));
   } else {
-    const long long pl = a.g.plane, d3 = a.g.d3;
-    const float xm = valo<kPassEnforce>(a, e, c, -1, 0, 0), xp = a.F[e + pl];
-    const float ym = valo<kPassEnforce>(a, e, c, 0, -1, 0), yp = a.F[e + d3];
-    const float zm = valo<kPassEnforce>(a, e, c, 0, 0, -1), zp = a.F[e + 1];
+    const float xm = valo<kPassEnforce>(a, e, c, -1, 0, 0), xp = pre_value(a, e, c, 1, 0, 0);
+    const float ym = valo<kPassEnforce>(a, e, c, 0, -1, 0), yp = pre_value(a, e, c, 0, 1, 0);
+    const float zm = valo<kPassEnforce>(a, e, c, 0, 0, -1), zp = pre_value(a, e, c, 0, 0, 1);
     m = (t == 1) ? fmaxf(fmaxf(xm, xp), fmaxf(fmaxf(ym, yp), fmaxf(zm, zp)))
                  : fminf(fminf(xm, xp), fminf(fminf(ym, yp), fminf(zm, zp)));
   }
@@ -582,6 +592,31 @@ __global__ void fn_detect_kernel(PostArgs a, const unsigned *__restrict__ Z, uns
   }
 }
 
+// One item of a pass (list index idx): its result goes to S, or it is
+// deferred (returns true) while an earlier candidate it reads is not final.
+template <int PASS, int ND>
+__device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx) {
+  const long long e = (long long)list[idx];
+  const C3 c = coords(a.g, e);
+  if (!deps_ready<PASS, ND>(a, e, c)) return true;
+  float r;
+  bool ok = false;
+  if (PASS == kPassStencil) {
+    const int t = ty(a, e);
+    const int s = (idx < a.n_sp) ? a.sp[idx] : 0;
+    r = (ND == 2) ? stencil2(a, e, c, t, s) : stencil3(a, e, c, t, s);
+  } else if (PASS == kPassEnforce) {
+    r = enforce<ND>(a, e, c, ty(a, e));
+  } else if (PASS == kPassRbf) {
+    r = (ND == 2) ? rbf2(a, e, c, ok) : rbf3(a, e, c, ok);
+  } else {
+    r = axis3(a, e, c, ok);
+  }
+  if (ok) atomicAdd(a.restored, 1u);
+  st_rlx(&a.S[e], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
+  return false;
+}
+
 // One round of a pass over a worklist of list indices (identity when W is
 // null).  Items whose earlier candidates are not final yet go to Wn.
 template <int PASS, int ND>
@@ -593,27 +628,7 @@ pass_round_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned 
   unsigned idx = 0;
   if (i < nw) {
     idx = W ? W[i] : i;
-    const long long e = (long long)list[idx];
-    const C3 c = coords(a.g, e);
-    if (!deps_ready<PASS, ND>(a, e, c)) {
-      defer = true;
-    } else {
-      float r;
-      bool ok = false;
-      if (PASS == kPassStencil) {
-        const int t = ty(a, e);
-        const int s = (idx < a.n_sp) ? a.sp[idx] : 0;
-        r = (ND == 2) ? stencil2(a, e, c, t, s) : stencil3(a, e, c, t, s);
-      } else if (PASS == kPassEnforce) {
-        r = enforce<ND>(a, e, c, ty(a, e));
-      } else if (PASS == kPassRbf) {
-        r = (ND == 2) ? rbf2(a, e, c, ok) : rbf3(a, e, c, ok);
-      } else {
-        r = axis3(a, e, c, ok);
-      }
-      if (ok) atomicAdd(a.restored, 1u);
-      st_rlx(&a.S[e], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
-    }
+    defer = pass_item<PASS, ND>(a, list, idx);
   }
   const unsigned m = __ballot_sync(0xffffffffu, defer);
   const int lane = threadIdx.x & 31;
@@ -631,6 +646,147 @@ __global__ void list_scatter_kernel(float *__restrict__ F, const unsigned long l
   if (i >= nlist) return;
   const long long e = (long long)list[sel ? sel[i] : i];
   F[e] = __uint_as_float((unsigned)S[e]);
+}
+
+// A round over a worklist whose length is on the device (*nw_dev), in a
+// grid-stride loop over a grid of any size (no barrier inside).
+template <int PASS, int ND>
+__global__ void __launch_bounds__(kPostThreads)
+pass_round_dev_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *__restrict__ W,
+                      const unsigned *nw_dev, unsigned *__restrict__ Wn, unsigned *wn_count) {
+  const unsigned nw = *nw_dev;
+  const int lane = threadIdx.x & 31;
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x; base < nw; base += stride) {
+    const unsigned i = base + threadIdx.x;
+    bool defer = false;
+    unsigned idx = 0;
+    if (i < nw) {
+      idx = W[i];
+      defer = pass_item<PASS, ND>(a, list, idx);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, defer);
+    unsigned wb = 0;
+    if (lane == 0 && m) wb = atomicAdd(wn_count, (unsigned)__popc(m));
+    wb = __shfl_sync(0xffffffffu, wb, 0);
+    if (defer) Wn[wb + __popc(m & ((1u << lane) - 1u))] = idx;
+  }
+}
+
+// Grid-wide barrier of a cooperative launch (every CTA resident): one
+// arrival counter and a generation word.  The last CTA to arrive resets the
+// counter and advances the generation; the others wait for the generation to
+// change.  The wait is bounded: after kBarSpinLimit polls the CTA records
+// kErrWaitTimeout and leaves the barrier (the pass then reports an error).
+constexpr int kBarSpinLimit = 1 << 22;
+
+__device__ __forceinline__ unsigned ld_acq_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_rel_u32(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const unsigned g = ld_acq_u32(bar + 1);
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      st_rel_u32(bar + 1, g + 1);
+    } else {
+      // exponential back-off keeps the pollers of all CTAs from crowding the
+      // generation word's L2 line while the last arrivals are still counting
+      int spins = 0;
+      unsigned nap = 64;
+      while (ld_acq_u32(bar + 1) == g) {
+        if (++spins > kBarSpinLimit) {
+          ok = 0;
+          atomicExch(err, kErrWaitTimeout);
+          break;
+        }
+        __nanosleep(nap);
+        if (nap < 1024) nap <<= 1;
+      }
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// The rounds of a pass after round 0 (or all of them), and the scatter of the
+// results into F, in one cooperative launch: rounds are separated by grid
+// barriers instead of host round trips.  The worklist starts as W_start with
+// *nstart_dev items (the deferred items of a round-0 launch) or, when W_start
+// is null, as sel (list indices; null = the whole list) with the pass's total
+// item count.  The total is *total_dev when that is not null, else total.
+// Worklists and counters written during the launch are read through L2
+// (__ldcg), since other SMs wrote them.  Every CTA takes the same branch at
+// every barrier: the counts it reads are final after the barrier.  With
+// scatter != 0 the results are copied into F at the end.
+// status: 0 done, 1 round limit, 2 no progress.
+constexpr int kCoopRoundLimit = 100000;
+
+template <int PASS, int ND>
+__global__ void __launch_bounds__(kPostThreads)
+pass_coop_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *sel, unsigned total,
+                 const unsigned *total_dev, const unsigned *W_start, const unsigned *nstart_dev, unsigned *Wx,
+                 unsigned *Wy, unsigned *cnts, unsigned *bar, unsigned long long *status, int scatter) {
+  const unsigned tot = total_dev ? __ldcg(total_dev) : total;
+  const unsigned *W = W_start ? W_start : sel;
+  unsigned nw = W_start ? __ldcg(nstart_dev) : tot;
+  const bool after_round0 = W_start != nullptr;
+  int b = 0;
+  const unsigned stride = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  for (int round = 0; nw > 0; round++) {
+    if (round >= kCoopRoundLimit) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) status[0] = 1;
+      return;
+    }
+    unsigned *Wn = b ? Wy : Wx;
+    // three counters in rotation: round r counts into cnts[r % 3].  The one
+    // the next round uses was last read before the barrier that ended round
+    // r - 1, which every CTA has passed once any CTA is in round r, so
+    // clearing it now cannot hide a count from a slower CTA.
+    unsigned *cnt = cnts + (round % 3);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(cnts + ((round + 1) % 3), 0u);
+    for (unsigned base = blockIdx.x * blockDim.x; base < nw; base += stride) {
+      const unsigned i = base + threadIdx.x;
+      bool defer = false;
+      unsigned idx = 0;
+      if (i < nw) {
+        idx = W ? __ldcg(W + i) : i;
+        defer = pass_item<PASS, ND>(a, list, idx);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, defer);
+      unsigned wb = 0;
+      if (lane == 0 && m) wb = atomicAdd(cnt, (unsigned)__popc(m));
+      wb = __shfl_sync(0xffffffffu, wb, 0);
+      if (defer) Wn[wb + __popc(m & ((1u << lane) - 1u))] = idx;
+    }
+    if (!grid_barrier(bar, a.err)) return;
+    const unsigned next = __ldcg(cnt);
+    if ((round > 0 || after_round0) && next >= nw) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) status[0] = 2;
+      return;
+    }
+    W = Wn;
+    nw = next;
+    b ^= 1;
+  }
+  if (!scatter) return;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += stride) {
+    const long long e = (long long)list[sel ? __ldcg(sel + i) : i];
+    a.F[e] = __uint_as_float((unsigned)ld_rlx(&a.S[e]));
+  }
 }
 
 // bits [b, b + 32) of a bitmap of nbits bits (zeros outside)
@@ -719,6 +875,68 @@ unsigned long long *post_words(szp_b200_ctx *ctx, unsigned long long n) {
   return ctx->post_S;
 }
 
+// Runs one pass without host round trips: round 0 as one full-width launch
+// (when the item count is known on the host), then the remaining rounds and
+// the scatter in one cooperative launch that reads its counts on the device.
+// Returns 1 when cooperative launch is not available (the caller then runs
+// the host-driven rounds).
+template <int PASS, int ND>
+static int run_pass_coop(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, const unsigned *sel,
+                         unsigned count, const unsigned *count_dev, unsigned *W0, unsigned *W1, int scatter = 1) {
+  static int grid_for_dev[64];
+  const int dev = ctx->device;
+  if (dev < 0 || dev >= 64) return 1;
+  if (grid_for_dev[dev] == 0) {
+    int coop = 0, nb = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pass_coop_kernel<PASS, ND>, kPostThreads, 0) !=
+            cudaSuccess ||
+        nb <= 0) {
+      cudaGetLastError();
+      grid_for_dev[dev] = -1;
+    } else {
+      grid_for_dev[dev] = nb * ctx->sm_count;
+    }
+  }
+  if (grid_for_dev[dev] < 0) return 1;
+  cudaStream_t s = ctx->stream;
+  // words 10..13: three round counters, the barrier counter and generation,
+  // the length of the round-1 worklist
+  unsigned *cnts = reinterpret_cast<unsigned *>(ctx->d_words + 10);
+  unsigned *bar = cnts + 3;
+  unsigned *n1 = cnts + 6;
+  unsigned *n0 = reinterpret_cast<unsigned *>(ctx->d_words + 7);
+  unsigned long long *status = ctx->d_words + 9;
+  if (cuda_fail(cudaMemsetAsync(cnts, 0, 32, s), "memset")) return -1;
+  const unsigned *W_start = nullptr, *nstart = nullptr;
+  unsigned *Wx = W0, *Wy = W1;
+  if (!count_dev) {
+    // rounds 0 and 1 as ordinary launches (all CTAs need not be resident:
+    // the big rounds balance better this way), the rest cooperatively
+    if (count == 0) return 0;
+    if (cuda_fail(cudaMemsetAsync(n0, 0, 4, s), "memset")) return -1;
+    pass_round_kernel<PASS, ND><<<(count + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(a, list, sel,
+                                                                                                count, W0, n0);
+    pass_round_dev_kernel<PASS, ND><<<ctx->sm_count * 8, kPostThreads, 0, s>>>(a, list, W0, n0, W1, n1);
+    ctx->launches += 2;
+    if (cuda_fail(cudaGetLastError(), "pass round")) return -1;
+    W_start = W1;
+    nstart = n1;
+    Wx = W0;
+    Wy = W1;
+  }
+  void *args[] = {(void *)&a,   (void *)&list,   (void *)&sel, (void *)&count, (void *)&count_dev,
+                  (void *)&W_start, (void *)&nstart, (void *)&Wx, (void *)&Wy, (void *)&cnts,
+                  (void *)&bar, (void *)&status, (void *)&scatter};
+  if (cuda_fail(cudaLaunchCooperativeKernel((const void *)pass_coop_kernel<PASS, ND>, dim3(grid_for_dev[dev]),
+                                            dim3(kPostThreads), args, 0, s),
+                "cooperative pass launch"))
+    return -1;
+  ctx->launches += 1;
+  return 0;
+}
+
 // Runs one pass in rounds over `list` (count items); returns 0 on success.
 template <int PASS, int ND>
 static int run_rounds(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, unsigned count,
@@ -791,13 +1009,23 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
                           const unsigned *Eb, const unsigned *Ib, int axis_stencil) {
   cudaStream_t s = ctx->stream;
   const long long n = a.n;
+  a.prev_in_S = false;
   if (a.sp && a.n_sp > 0) {
+    // the stencil results stay in S: enforcement runs over the same list and
+    // reads its candidates' pre-pass values there, so F is written once
     a.gen = next_gen(ctx);
-    if (run_rounds<kPassStencil, ND>(ctx, a, X, nx, W0, W1, nullptr)) return -1;
+    const int rc = run_pass_coop<kPassStencil, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1, 0);
+    if (rc < 0) return -1;
+    if (rc > 0 && run_rounds<kPassStencil, ND>(ctx, a, X, nx, W0, W1, nullptr)) return -1;
+    a.prev_in_S = rc == 0;
     tl_mark(ctx, "post_stencil");
   }
   a.gen = next_gen(ctx);
-  if (run_rounds<kPassEnforce, ND>(ctx, a, X, nx, W0, W1, nullptr)) return -1;
+  {
+    const int rc = run_pass_coop<kPassEnforce, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
+    if (rc < 0 || (rc > 0 && run_rounds<kPassEnforce, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
+  }
+  a.prev_in_S = false;
   tl_mark(ctx, "post_enforce");
   // locks (static: from the types) and the lost saddles (from F after enforcement)
   const long long words = (n + 31) / 32;
@@ -809,21 +1037,25 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   a.R = R;
   if (nz) fn_detect_kernel<<<(nz + 255) / 256, 256, 0, s>>>(a, Z, nz, R, Y, ycnt);
   ctx->launches += 2;
-  unsigned ny = 0;
-  if (cuda_fail(cudaGetLastError(), "fn detect") ||
-      cuda_fail(cudaMemcpyAsync(&ny, ycnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
-      cuda_fail(cudaStreamSynchronize(s), "fn detect"))
-    return -1;
+  if (cuda_fail(cudaGetLastError(), "fn detect")) return -1;
   tl_mark(ctx, "post_fn_locks");
-  if (ny) {
-    // RBF runs over Z restricted to the lost saddles (Y holds indices into Z)
-    a.gen = next_gen(ctx);
-    if (run_rounds_sel<kPassRbf, ND>(ctx, a, Z, Y, ny, W0, W1)) return -1;
+  // RBF runs over Z restricted to the lost saddles (Y holds indices into Z);
+  // their number stays on the device
+  a.gen = next_gen(ctx);
+  const int rc = nz ? run_pass_coop<kPassRbf, ND>(ctx, a, Z, Y, 0, ycnt, W0, W1) : 0;
+  if (rc < 0) return -1;
+  if (rc > 0) {
+    unsigned ny = 0;
+    if (cuda_fail(cudaMemcpyAsync(&ny, ycnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+        cuda_fail(cudaStreamSynchronize(s), "fn detect"))
+      return -1;
+    if (ny && run_rounds_sel<kPassRbf, ND>(ctx, a, Z, Y, ny, W0, W1)) return -1;
   }
   tl_mark(ctx, "post_rbf");
   if (axis_stencil && ND == 3 && nz) {
     a.gen = next_gen(ctx);
-    if (run_rounds<kPassAxis, ND>(ctx, a, Z, nz, W0, W1, nullptr)) return -1;
+    const int ra = run_pass_coop<kPassAxis, ND>(ctx, a, Z, nullptr, nz, nullptr, W0, W1);
+    if (ra < 0 || (ra > 0 && run_rounds<kPassAxis, ND>(ctx, a, Z, nz, W0, W1, nullptr))) return -1;
     tl_mark(ctx, "post_axis");
   }
   return 0;
@@ -849,8 +1081,8 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
     set_error("scratch arena too small for post-processing");
     return -1;
   }
-  unsigned long long *w = ctx->d_words;
-  if (cuda_fail(cudaMemsetAsync(w, 0, 80, s), "memset")) return -1;
+  unsigned long long *w = ctx->d_words;  // [9] pass status, [10] round counters
+  if (cuda_fail(cudaMemsetAsync(w, 0, 96, s), "memset")) return -1;
   const long long ntiles = (n + kPostTile - 1) / kPostTile;
   // per-tile counts live in the descriptor buffer (32 bytes per tile available)
   unsigned long long *tcnt = reinterpret_cast<unsigned long long *>(desc);
@@ -891,11 +1123,13 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   const int rc = (g.nd == 2) ? run_all_passes<2>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, axis_stencil)
                              : run_all_passes<3>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, axis_stencil);
   if (rc) return -1;
-  if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 80, cudaMemcpyDeviceToHost, s), "D2H") ||
+  if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 96, cudaMemcpyDeviceToHost, s), "D2H") ||
       cuda_fail(cudaStreamSynchronize(s), "postprocess"))
     return -1;
   const int err = (int)(ctx->h_words[4] & 0xffffffffu);
   if (err) { set_error("post-processing status %d", err); return -1; }
+  if (ctx->h_words[9] == 1) { set_error("post-processing pass did not converge"); return -1; }
+  if (ctx->h_words[9] == 2) { set_error("post-processing pass made no progress"); return -1; }
   if (restored_out) *restored_out = (int)(ctx->h_words[5] & 0xffffffffu);
   return 0;
 }
