@@ -570,6 +570,92 @@ list_write_kernel(const unsigned char *__restrict__ T, Geom g, long long n, cons
   }
 }
 
+// Interior extrema (X) and interior saddles (Z) in raster order plus the two
+// bitmaps (extrema Eb, interior Ib), in one pass over the types: persistent
+// CTAs take tiles of kPostTile points in order, publish their counts and find
+// their list offsets by decoupled look-back (extrema in the byte word, saddles
+// in the count word), then write their entries through shared memory so each
+// tile's slice of X and Z is stored contiguously.  The last tile writes the
+// totals to tot[0] = (extrema << 32) | saddles.
+__global__ void __launch_bounds__(kPostThreads)
+list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, TileDesc *desc, unsigned *tile_ctr,
+                  int *err, unsigned *X, unsigned *Z, unsigned char *Eb, unsigned char *Ib,
+                  unsigned long long *tot) {
+  __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
+  __shared__ unsigned s_x[kPostTile], s_z[kPostTile];
+  __shared__ long long s_tile;
+  __shared__ unsigned long long s_xb, s_zb;
+  const long long ntiles = (n + kPostTile - 1) / kPostTile;
+  while (true) {
+    if (threadIdx.x == 0) s_tile = (long long)atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    const long long tile = s_tile;
+    if (tile >= ntiles) break;
+    const long long i0 = tile * kPostTile + (long long)threadIdx.x * kPostPer;
+    unsigned em = 0, sm = 0, im = 0;
+    if (i0 < n) {
+      long long r, x, y, z;
+      if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
+      else { x = fdivmod(i0, g.plane, g.m_plane, r); y = fdivmod(r, g.d3, g.m_d3, z); }
+      unsigned long long w = 0;
+      if (i0 + 8 <= n && ((reinterpret_cast<uintptr_t>(T + i0) & 7) == 0)) {
+        w = *reinterpret_cast<const unsigned long long *>(T + i0);
+      } else {
+        for (int u = 0; u < 8; u++) if (i0 + u < n) w |= (unsigned long long)T[i0 + u] << (8 * u);
+      }
+      if (z + 7 < g.d3 && i0 + 8 <= n) {
+        // the 8 points share one row: interior columns 1 .. d3-2
+        const bool row_in = y >= 1 && y <= g.d2 - 2 && (g.nd == 2 || (x >= 1 && x <= g.d1 - 2));
+        if (row_in) {
+          const long long lo = 1 - z, hi = g.d3 - 2 - z;   // interior offsets u in [lo, hi]
+          const int ulo = lo > 0 ? (int)lo : 0, uhi = hi < 7 ? (int)hi : 7;
+          if (ulo <= uhi) im = ((2u << uhi) - 1u) & ~((1u << ulo) - 1u);
+        }
+      } else {
+        for (int u = 0; u < kPostPer && i0 + u < n; u++) {
+          bool in = y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
+          if (g.nd == 3) in = in && x >= 1 && x <= g.d1 - 2;
+          if (in) im |= 1u << u;
+          z++;
+          while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kPostPer; u++) {
+        const unsigned t = (unsigned)(w >> (8 * u)) & 3u;
+        if ((im >> u) & 1u) {
+          if (t == 1u || t == 2u) em |= 1u << u;
+          if (t == 3u) sm |= 1u << u;
+        }
+      }
+      Eb[i0 >> 3] = (unsigned char)em;
+      Ib[i0 >> 3] = (unsigned char)im;
+    }
+    unsigned te, ts;
+    const unsigned eo = cta_excl_scan_post((unsigned)__popc(em), s_w1, &te);
+    const unsigned so = cta_excl_scan_post((unsigned)__popc(sm), s_w2, &ts);
+    if (threadIdx.x == 0) publish_aggregate(desc, tile, te, ts);
+    {
+      unsigned xe = eo, xs = so;
+      for (int u = 0; u < kPostPer; u++) {
+        if (em & (1u << u)) s_x[xe++] = (unsigned)(i0 + u);
+        if (sm & (1u << u)) s_z[xs++] = (unsigned)(i0 + u);
+      }
+    }
+    const Prefix pf = lookback_cta<kWarps>(desc, tile, te, ts, err);
+    if (threadIdx.x == 0) {
+      s_xb = pf.bytes;
+      s_zb = pf.cnt;
+      if (tile == ntiles - 1) *tot = ((pf.bytes + te) << 32) | (pf.cnt + ts);
+    }
+    __syncthreads();
+    const unsigned long long xb = s_xb, zb = s_zb;
+    for (unsigned k = threadIdx.x; k < te; k += kPostThreads) X[xb + k] = s_x[k];
+    for (unsigned k = threadIdx.x; k < ts; k += kPostThreads) Z[zb + k] = s_z[k];
+    __syncthreads();
+  }
+}
+
 // lost saddles (RBF candidates): saddles of the original field that F no
 // longer classifies as saddles (example/test_cuda_topology.cu:244-254)
 __global__ void fn_detect_kernel(PostArgs a, const unsigned *__restrict__ Z, unsigned long long nz,
@@ -1084,8 +1170,6 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   unsigned long long *w = ctx->d_words;  // [9] pass status, [10] round counters
   if (cuda_fail(cudaMemsetAsync(w, 0, 96, s), "memset")) return -1;
   const long long ntiles = (n + kPostTile - 1) / kPostTile;
-  // per-tile counts live in the descriptor buffer (32 bytes per tile available)
-  unsigned long long *tcnt = reinterpret_cast<unsigned long long *>(desc);
   {
     // the words past the last written byte of the two bitmaps must read as zero
     const long long words = (n + 31) / 32;
@@ -1093,15 +1177,19 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
         cuda_fail(cudaMemsetAsync(Ib + words - 1, 0, 8, s), "memset"))
       return -1;
   }
-  list_count_kernel<<<(unsigned)ntiles, kPostThreads, 0, s>>>(d_T, g, n, tcnt);
-  list_scan_kernel<<<1, 1024, 0, s>>>(tcnt, ntiles);
-  list_write_kernel<<<(unsigned)ntiles, kPostThreads, 0, s>>>(d_T, g, n, tcnt, X, Z,
-                                                            reinterpret_cast<unsigned char *>(Eb),
-                                                            reinterpret_cast<unsigned char *>(Ib));
-  ctx->launches += 3;
+  unsigned *tile_ctr = reinterpret_cast<unsigned *>(w + 3);
+  unsigned long long *d_tot = w + 2;
+  if (cuda_fail(cudaMemsetAsync(desc, 0, (ntiles + 1) * sizeof(TileDesc), s), "memset")) return -1;
+  {
+    const unsigned grid = (unsigned)std::min<long long>(ntiles, (long long)ctx->sm_count * 8);
+    list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
+                                                    Z, reinterpret_cast<unsigned char *>(Eb),
+                                                    reinterpret_cast<unsigned char *>(Ib), d_tot);
+  }
+  ctx->launches += 1;
   unsigned long long tot = 0;
   if (cuda_fail(cudaGetLastError(), "lists") ||
-      cuda_fail(cudaMemcpyAsync(&tot, tcnt + ntiles, 8, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaMemcpyAsync(&tot, d_tot, 8, cudaMemcpyDeviceToHost, s), "D2H") ||
       cuda_fail(cudaStreamSynchronize(s), "lists"))
     return -1;
   const unsigned nx = (unsigned)(tot >> 32), nz = (unsigned)(tot & 0xffffffffull);
