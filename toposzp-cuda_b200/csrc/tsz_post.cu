@@ -572,47 +572,46 @@ list_write_kernel(const unsigned char *__restrict__ T, Geom g, long long n, cons
 
 // Interior extrema (X) and interior saddles (Z) in raster order plus the two
 // bitmaps (extrema Eb, interior Ib), in one pass over the types: persistent
-// CTAs take tiles of kPostTile points in order, publish their counts and find
-// their list offsets by decoupled look-back (extrema in the byte word, saddles
-// in the count word), then write their entries through shared memory so each
-// tile's slice of X and Z is stored contiguously.  The last tile writes the
-// totals to tot[0] = (extrema << 32) | saddles.
+// CTAs take tiles of kListTile points in order (32 consecutive points per
+// thread), publish their counts and find their list offsets by decoupled
+// look-back (extrema in the byte word, saddles in the count word), then write
+// their entries through shared memory so each tile's slice of X and Z is
+// stored contiguously (X staged from the front of one buffer, Z from its back:
+// a point is in at most one list).  The last tile writes the totals to
+// tot[0] = (extrema << 32) | saddles.
+constexpr int kListPer = 32;
+constexpr int kListTile = kPostThreads * kListPer;
+
 __global__ void __launch_bounds__(kPostThreads)
 list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, TileDesc *desc, unsigned *tile_ctr,
                   int *err, unsigned *X, unsigned *Z, unsigned char *Eb, unsigned char *Ib,
                   unsigned long long *tot) {
   __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
-  __shared__ unsigned s_x[kPostTile], s_z[kPostTile];
+  __shared__ unsigned s_buf[kListTile];
   __shared__ long long s_tile;
   __shared__ unsigned long long s_xb, s_zb;
-  const long long ntiles = (n + kPostTile - 1) / kPostTile;
+  const long long ntiles = (n + kListTile - 1) / kListTile;
   while (true) {
     if (threadIdx.x == 0) s_tile = (long long)atomicAdd(tile_ctr, 1u);
     __syncthreads();
     const long long tile = s_tile;
     if (tile >= ntiles) break;
-    const long long i0 = tile * kPostTile + (long long)threadIdx.x * kPostPer;
+    const long long i0 = tile * kListTile + (long long)threadIdx.x * kListPer;
     unsigned em = 0, sm = 0, im = 0;
     if (i0 < n) {
       long long r, x, y, z;
       if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
       else { x = fdivmod(i0, g.plane, g.m_plane, r); y = fdivmod(r, g.d3, g.m_d3, z); }
-      unsigned long long w = 0;
-      if (i0 + 8 <= n && ((reinterpret_cast<uintptr_t>(T + i0) & 7) == 0)) {
-        w = *reinterpret_cast<const unsigned long long *>(T + i0);
-      } else {
-        for (int u = 0; u < 8; u++) if (i0 + u < n) w |= (unsigned long long)T[i0 + u] << (8 * u);
-      }
-      if (z + 7 < g.d3 && i0 + 8 <= n) {
-        // the 8 points share one row: interior columns 1 .. d3-2
+      if (z + kListPer - 1 < g.d3 && i0 + kListPer <= n) {
+        // the 32 points share one row: interior columns 1 .. d3-2
         const bool row_in = y >= 1 && y <= g.d2 - 2 && (g.nd == 2 || (x >= 1 && x <= g.d1 - 2));
         if (row_in) {
           const long long lo = 1 - z, hi = g.d3 - 2 - z;   // interior offsets u in [lo, hi]
-          const int ulo = lo > 0 ? (int)lo : 0, uhi = hi < 7 ? (int)hi : 7;
-          if (ulo <= uhi) im = ((2u << uhi) - 1u) & ~((1u << ulo) - 1u);
+          const int ulo = lo > 0 ? (int)lo : 0, uhi = hi < kListPer - 1 ? (int)hi : kListPer - 1;
+          if (ulo <= uhi) im = (uhi == 31 ? 0xffffffffu : ((2u << uhi) - 1u)) & ~((1u << ulo) - 1u);
         }
       } else {
-        for (int u = 0; u < kPostPer && i0 + u < n; u++) {
+        for (int u = 0; u < kListPer && i0 + u < n; u++) {
           bool in = y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
           if (g.nd == 3) in = in && x >= 1 && x <= g.d1 - 2;
           if (in) im |= 1u << u;
@@ -620,16 +619,42 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
           while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
         }
       }
+      if (im) {
+        const bool vec = i0 + kListPer <= n && ((reinterpret_cast<uintptr_t>(T + i0) & 15) == 0);
 #pragma unroll
-      for (int u = 0; u < kPostPer; u++) {
-        const unsigned t = (unsigned)(w >> (8 * u)) & 3u;
-        if ((im >> u) & 1u) {
-          if (t == 1u || t == 2u) em |= 1u << u;
-          if (t == 3u) sm |= 1u << u;
+        for (int h = 0; h < 2; h++) {
+          unsigned long long w0 = 0, w1 = 0;
+          if (vec) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4 *>(T + i0) + h);
+            w0 = ((unsigned long long)v.y << 32) | v.x;
+            w1 = ((unsigned long long)v.w << 32) | v.z;
+          } else {
+            for (int u = 0; u < 8; u++) {
+              if (i0 + 16 * h + u < n) w0 |= (unsigned long long)T[i0 + 16 * h + u] << (8 * u);
+              if (i0 + 16 * h + 8 + u < n) w1 |= (unsigned long long)T[i0 + 16 * h + 8 + u] << (8 * u);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 16; u++) {
+            const unsigned t = (unsigned)((u < 8 ? w0 : w1) >> (8 * (u & 7))) & 3u;
+            const unsigned bit = 1u << (16 * h + u);
+            if (im & bit) {
+              if (t == 1u || t == 2u) em |= bit;
+              if (t == 3u) sm |= bit;
+            }
+          }
         }
       }
-      Eb[i0 >> 3] = (unsigned char)em;
-      Ib[i0 >> 3] = (unsigned char)im;
+      // 4 bitmap bytes of this thread's 32 points (i0 is a multiple of 32)
+      if (i0 + kListPer <= n) {
+        reinterpret_cast<unsigned *>(Eb)[i0 >> 5] = em;
+        reinterpret_cast<unsigned *>(Ib)[i0 >> 5] = im;
+      } else {
+        for (int k = 0; k < 4 && i0 + 8 * k < n; k++) {
+          Eb[(i0 >> 3) + k] = (unsigned char)(em >> (8 * k));
+          Ib[(i0 >> 3) + k] = (unsigned char)(im >> (8 * k));
+        }
+      }
     }
     unsigned te, ts;
     const unsigned eo = cta_excl_scan_post((unsigned)__popc(em), s_w1, &te);
@@ -637,10 +662,10 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
     if (threadIdx.x == 0) publish_aggregate(desc, tile, te, ts);
     {
       unsigned xe = eo, xs = so;
-      for (int u = 0; u < kPostPer; u++) {
-        if (em & (1u << u)) s_x[xe++] = (unsigned)(i0 + u);
-        if (sm & (1u << u)) s_z[xs++] = (unsigned)(i0 + u);
-      }
+      unsigned mm = em;
+      while (mm) { const int u = __ffs(mm) - 1; mm &= mm - 1; s_buf[xe++] = (unsigned)(i0 + u); }
+      mm = sm;
+      while (mm) { const int u = __ffs(mm) - 1; mm &= mm - 1; s_buf[kListTile - 1 - xs++] = (unsigned)(i0 + u); }
     }
     const Prefix pf = lookback_cta<kWarps>(desc, tile, te, ts, err);
     if (threadIdx.x == 0) {
@@ -650,8 +675,8 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
     }
     __syncthreads();
     const unsigned long long xb = s_xb, zb = s_zb;
-    for (unsigned k = threadIdx.x; k < te; k += kPostThreads) X[xb + k] = s_x[k];
-    for (unsigned k = threadIdx.x; k < ts; k += kPostThreads) Z[zb + k] = s_z[k];
+    for (unsigned k = threadIdx.x; k < te; k += kPostThreads) X[xb + k] = s_buf[k];
+    for (unsigned k = threadIdx.x; k < ts; k += kPostThreads) Z[zb + k] = s_buf[kListTile - 1 - k];
     __syncthreads();
   }
 }
@@ -1179,9 +1204,10 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   }
   unsigned *tile_ctr = reinterpret_cast<unsigned *>(w + 3);
   unsigned long long *d_tot = w + 2;
-  if (cuda_fail(cudaMemsetAsync(desc, 0, (ntiles + 1) * sizeof(TileDesc), s), "memset")) return -1;
+  const long long ltiles = (n + kListTile - 1) / kListTile;
+  if (cuda_fail(cudaMemsetAsync(desc, 0, (ltiles + 1) * sizeof(TileDesc), s), "memset")) return -1;
   {
-    const unsigned grid = (unsigned)std::min<long long>(ntiles, (long long)ctx->sm_count * 8);
+    const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 4);
     list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
                                                     Z, reinterpret_cast<unsigned char *>(Eb),
                                                     reinterpret_cast<unsigned char *>(Ib), d_tot);
