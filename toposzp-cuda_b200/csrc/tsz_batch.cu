@@ -278,7 +278,7 @@ __global__ void batch_sort_header_kernel(const BatchHdr *hdr, const EncArgs *arg
 template <int MODE, int WARPS>
 static size_t batch_smem(int B) {
   const int tb = WARPS * (32 / octet_group(B));
-  return (((size_t)tb * max_block_bytes((uint32_t)B, MODE != kEncInts) + 64) + 15) & ~(size_t)15;
+  return enc2_total_smem(B, MODE != kEncInts, MODE == kEncClassify, WARPS, tb);
 }
 
 // prepare == true sets the kernel's shared-memory limit (outside any stream

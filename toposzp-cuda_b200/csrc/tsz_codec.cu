@@ -544,15 +544,15 @@ int octet_group(int B) {
   return g;
 }
 
-size_t enc2_smem_bytes(int B, bool tags) {
+size_t enc2_smem_bytes(int B, bool tags, bool classify) {
   const int tb = kWarps * (32 / octet_group(B));
-  return (((size_t)tb * max_block_bytes((uint32_t)B, tags) + 64) + 15) & ~(size_t)15;
+  return enc2_total_smem(B, tags, classify, kWarps, tb);
 }
 
 template <int MODE, int G>
 static cudaError_t launch_enc2(const EncArgs &a, cudaStream_t s, int grid) {
   auto k = encode2_kernel<MODE, G>;
-  const size_t sm = enc2_smem_bytes(a.B, MODE != kEncInts);
+  const size_t sm = enc2_smem_bytes(a.B, MODE != kEncInts, MODE == kEncClassify);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   k<<<grid, kThreads, sm, s>>>(a);

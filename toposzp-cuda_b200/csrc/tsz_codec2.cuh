@@ -14,6 +14,16 @@
 
 namespace tsz {
 
+// Dynamic shared memory of an encoder CTA: the tile image (tb blocks at their
+// largest size) followed, in classification mode, by the staging area of the
+// tile's critical-point pairs (one uint2 per point of the tile).
+__host__ __device__ __forceinline__ unsigned enc2_img_bytes(int B, bool tags, int tb) {
+  return ((unsigned)tb * max_block_bytes((uint32_t)B, tags) + 64u + 15u) & ~15u;
+}
+__host__ __device__ __forceinline__ unsigned enc2_total_smem(int B, bool tags, bool classify, int warps, int tb) {
+  return enc2_img_bytes(B, tags, tb) + (classify ? (unsigned)warps * 256u * 8u : 0u);
+}
+
 // loads 8 floats at p[i..i+7]: one 32-byte vector load when aligned and fully
 // in range, otherwise scalar loads for the elements selected by need
 __device__ __forceinline__ void load_oct(const float *__restrict__ p, long long i, long long n,
@@ -40,14 +50,25 @@ __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, 
   if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
   else { x = fdivmod(i0, g.plane, g.m_plane, r); y = fdivmod(r, g.d3, g.m_d3, z); }
   unsigned inter = 0;
+  if (z + 7 < g.d3) {
+    // the octet lies in one row: interior columns 1 .. d3-2
+    const bool row_in = y >= 1 && y <= g.d2 - 2 && (g.nd == 2 || (x >= 1 && x <= g.d1 - 2));
+    if (row_in) {
+      const long long lo = 1 - z, hi = g.d3 - 2 - z;
+      const int ulo = lo > 0 ? (int)lo : 0, uhi = hi < 7 ? (int)hi : 7;
+      if (ulo <= uhi) inter = ((2u << uhi) - 1u) & ~((1u << ulo) - 1u);
+    }
+    inter &= (nv >= 8) ? 0xffu : ((1u << nv) - 1u);
+  } else {
 #pragma unroll
-  for (int t = 0; t < 8; t++) {
-    const bool in = t < nv;
-    bool ok = in && y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
-    if (g.nd == 3) ok = ok && x >= 1 && x <= g.d1 - 2;
-    if (ok) inter |= 1u << t;
-    z++;
-    while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
+    for (int t = 0; t < 8; t++) {
+      const bool in = t < nv;
+      bool ok = in && y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
+      if (g.nd == 3) ok = ok && x >= 1 && x <= g.d1 - 2;
+      if (ok) inter |= 1u << t;
+      z++;
+      while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
+    }
   }
   if (inter == 0) return 0u;
   // +-1 neighbours: inside the octet, plus one scalar load at each end
@@ -266,6 +287,19 @@ __device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long t
     }
     __syncthreads();
     const unsigned tile_bytes = sh.tile_bytes;
+    // critical-point pairs of the tile, staged in thread (= raster) order;
+    // extremum indices tile-local until the look-back gives the base
+    uint2 *cp_stage = reinterpret_cast<uint2 *>(img + enc2_img_bytes(B, tags, TB));
+    if (MODE == kEncClassify && a.cp_mode == kCpPairs && cpm) {
+      unsigned ci = cpo, ei = exo;
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        if (!(cpm & (1u << t))) continue;
+        const unsigned ty = (types >> (2 * t)) & 3u;
+        const bool ext = (ty == 1u || ty == 2u);
+        cp_stage[ci++] = make_uint2(float_code(x[t]), ext ? ei++ : kNoExtremum);
+      }
+    }
 
     // ---- phase 3: pack the octet into the tile image ----
     if (a.out != nullptr && nv > 0) {
@@ -392,7 +426,18 @@ __device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long t
     }
 
     // ---- phase 6: critical points in raster order (thread order == raster order) ----
-    if (MODE == kEncClassify && a.cp_mode != kCpNone && cpm) {
+    if (MODE == kEncClassify && a.cp_mode == kCpPairs) {
+      const unsigned long long cb = sh.gcnt >> 32;
+      const uint32_t eb0 = (uint32_t)(sh.gcnt & 0xffffffffull);
+      const unsigned ntc = sh.tile_cps;
+      for (unsigned k = threadIdx.x; k < ntc; k += WARPS * 32) {
+        if (cb + k < a.cp_cap) {
+          uint2 pr = cp_stage[k];
+          if (pr.y != kNoExtremum) pr.y += eb0;
+          reinterpret_cast<uint2 *>(a.cp_out)[cb + k] = pr;
+        }
+      }
+    } else if (MODE == kEncClassify && a.cp_mode == kCpRecords && cpm) {
       unsigned long long ci = (sh.gcnt >> 32) + cpo;
       unsigned long long ei = (sh.gcnt & 0xffffffffull) + exo;
 #pragma unroll
