@@ -297,7 +297,7 @@ __device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long t
         if (!(cpm & (1u << t))) continue;
         const unsigned ty = (types >> (2 * t)) & 3u;
         const bool ext = (ty == 1u || ty == 2u);
-        cp_stage[ci++] = make_uint2(float_code(x[t]), ext ? ei++ : kNoExtremum);
+        cp_stage[ci++] = make_uint2(float_code(__ldg(a.data + i0 + t)), ext ? ei++ : kNoExtremum);
       }
     }
 
