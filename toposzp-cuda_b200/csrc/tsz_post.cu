@@ -397,23 +397,25 @@ __device__ bool valid3(const PostArgs &a, long long e, const C3 &c, Win3 &W, flo
   return true;
 }
 
-// 3D RBF (example/test_cuda_topology_3d.cu:317-434)
+// 3D RBF (example/test_cuda_topology_3d.cu:317-434).  Every value the
+// validation can read is loaded once into registers (compile-time indices):
+// the 3x3x3 box around e and the points two steps out along each axis, the
+// latter only where the serial code would read them (the neighbour on that
+// side is interior and regular).  A trial changes only the centre value.
 __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
   ok = false;
-  Win3 W;
-  W.c = c;
-  for (int i = 0; i < 125; i++) (&W.have[0][0][0])[i] = 0;
   const float old = a.F[e];
+  float v[27];   // box value at (dx, dy, dz): v[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)]
   double num = 0.0, den = 0.0;
-  for (int da = -1; da <= 1; da++)
-    for (int db = -1; db <= 1; db++)
-      for (int dc = -1; dc <= 1; dc++) {
-        double ww = c_w3[(da + 1) * 9 + (db + 1) * 3 + (dc + 1)];
-        if (locked(a, e + da * a.g.plane + db * a.g.d3 + dc)) ww = __dmul_rn(ww, 0.4);
-        const float v = w3getp<kPassRbf>(a, e, W, da, db, dc, old);
-        num = __dadd_rn(num, __dmul_rn(ww, (double)v));
-        den = __dadd_rn(den, ww);
-      }
+#pragma unroll
+  for (int i = 0; i < 27; i++) {
+    const int dx = i / 9 - 1, dy = (i / 3) % 3 - 1, dz = i % 3 - 1;
+    v[i] = (i == 13) ? old : valo<kPassRbf>(a, e, c, dx, dy, dz);
+    double ww = c_w3[i];
+    if (locked(a, e + dx * a.g.plane + dy * a.g.d3 + dz)) ww = __dmul_rn(ww, 0.4);
+    num = __dadd_rn(num, __dmul_rn(ww, (double)v[i]));
+    den = __dadd_rn(den, ww);
+  }
   if (!(den > 0.0)) return old;
   const float o = a.O[e];
   const float d = __fmul_rn(a.eb, 0.999f);
@@ -421,15 +423,42 @@ __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
   float cand = __double2float_rn(__ddiv_rn(num, den));
   if (cand < lo) cand = lo;
   if (cand > hi) cand = hi;
+  // neighbours whose classification the validation checks, and their far sides
+  const long long pl = a.g.plane, d3 = a.g.d3;
+  const bool cxm = c.x - 1 >= 1 && ty(a, e - pl) == 0, cxp = c.x + 1 < a.g.d1 - 1 && ty(a, e + pl) == 0;
+  const bool cym = c.y - 1 >= 1 && ty(a, e - d3) == 0, cyp = c.y + 1 < a.g.d2 - 1 && ty(a, e + d3) == 0;
+  const bool czm = c.z - 1 >= 1 && ty(a, e - 1) == 0, czp = c.z + 1 < a.g.d3 - 1 && ty(a, e + 1) == 0;
+  const float fxm = cxm ? valo<kPassRbf>(a, e, c, -2, 0, 0) : 0.f;
+  const float fxp = cxp ? valo<kPassRbf>(a, e, c, 2, 0, 0) : 0.f;
+  const float fym = cym ? valo<kPassRbf>(a, e, c, 0, -2, 0) : 0.f;
+  const float fyp = cyp ? valo<kPassRbf>(a, e, c, 0, 2, 0) : 0.f;
+  const float fzm = czm ? valo<kPassRbf>(a, e, c, 0, 0, -2) : 0.f;
+  const float fzp = czp ? valo<kPassRbf>(a, e, c, 0, 0, 2) : 0.f;
+#define V3(dx, dy, dz) v[((dx) + 1) * 9 + ((dy) + 1) * 3 + ((dz) + 1)]
   const float step = __fsub_rn(cand, old);
   float alpha = 1.0f;
   for (int it = 0; it < 10; it++) {
-    float trial = __fadd_rn(old, __fmul_rn(alpha, step));
-    if (trial < lo) trial = lo;
-    if (trial > hi) trial = hi;
-    if (valid3<kPassRbf>(a, e, c, W, trial)) { ok = true; return trial; }
+    float tr = __fadd_rn(old, __fmul_rn(alpha, step));
+    if (tr < lo) tr = lo;
+    if (tr > hi) tr = hi;
+    // classify6(centre, x-, x+, y-, y+, z-, z+) of the centre and of each checked neighbour
+    bool good = classify6(tr, V3(-1, 0, 0), V3(1, 0, 0), V3(0, -1, 0), V3(0, 1, 0), V3(0, 0, -1), V3(0, 0, 1)) == 3;
+    if (good && cxm)
+      good = classify6(V3(-1, 0, 0), fxm, tr, V3(-1, -1, 0), V3(-1, 1, 0), V3(-1, 0, -1), V3(-1, 0, 1)) == 0;
+    if (good && cxp)
+      good = classify6(V3(1, 0, 0), tr, fxp, V3(1, -1, 0), V3(1, 1, 0), V3(1, 0, -1), V3(1, 0, 1)) == 0;
+    if (good && cym)
+      good = classify6(V3(0, -1, 0), V3(-1, -1, 0), V3(1, -1, 0), fym, tr, V3(0, -1, -1), V3(0, -1, 1)) == 0;
+    if (good && cyp)
+      good = classify6(V3(0, 1, 0), V3(-1, 1, 0), V3(1, 1, 0), tr, fyp, V3(0, 1, -1), V3(0, 1, 1)) == 0;
+    if (good && czm)
+      good = classify6(V3(0, 0, -1), V3(-1, 0, -1), V3(1, 0, -1), V3(0, -1, -1), V3(0, 1, -1), fzm, tr) == 0;
+    if (good && czp)
+      good = classify6(V3(0, 0, 1), V3(-1, 0, 1), V3(1, 0, 1), V3(0, -1, 1), V3(0, 1, 1), tr, fzp) == 0;
+    if (good) { ok = true; return tr; }
     alpha = __fmul_rn(alpha, 0.5f);
   }
+#undef V3
   return old;
 }
 
