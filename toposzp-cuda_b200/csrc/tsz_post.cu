@@ -757,6 +757,28 @@ __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__r
   return false;
 }
 
+// An item whose earlier candidate is handled by the same CTA at the same
+// time (the previous point of a row, or of the previous row) would be
+// deferred to the next round; the CTA instead retries its pending items a
+// few times, a block barrier apart, so that chains inside the CTA resolve in
+// this round.  Every thread of the CTA must call it.  Returns true while the
+// item is still pending.
+constexpr int kLocalRetries = 4;
+
+template <int PASS, int ND>
+__device__ __forceinline__ bool pass_item_local(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx,
+                                                bool valid) {
+  // RBF and axis-pattern items are long and uneven: a block barrier would make
+  // every thread wait for the slowest, so they retry in rounds only
+  if (PASS != kPassStencil && PASS != kPassEnforce) return valid && pass_item<PASS, ND>(a, list, idx);
+  bool pending = valid;
+  for (int it = 0; it < kLocalRetries; it++) {
+    if (pending) pending = pass_item<PASS, ND>(a, list, idx);
+    if (!__syncthreads_or(pending)) break;
+  }
+  return pending;
+}
+
 // One round of a pass over a worklist of list indices (identity when W is
 // null).  Items whose earlier candidates are not final yet go to Wn.
 template <int PASS, int ND>
@@ -764,12 +786,9 @@ __global__ void __launch_bounds__(kPostThreads)
 pass_round_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *__restrict__ W,
                   unsigned nw, unsigned *__restrict__ Wn, unsigned *wn_count) {
   const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool defer = false;
   unsigned idx = 0;
-  if (i < nw) {
-    idx = W ? W[i] : i;
-    defer = pass_item<PASS, ND>(a, list, idx);
-  }
+  if (i < nw) idx = W ? W[i] : i;
+  const bool defer = pass_item_local<PASS, ND>(a, list, idx, i < nw);
   const unsigned m = __ballot_sync(0xffffffffu, defer);
   const int lane = threadIdx.x & 31;
   unsigned base = 0;
@@ -799,12 +818,9 @@ pass_round_dev_kernel(PostArgs a, const unsigned *__restrict__ list, const unsig
   const unsigned stride = gridDim.x * blockDim.x;
   for (unsigned base = blockIdx.x * blockDim.x; base < nw; base += stride) {
     const unsigned i = base + threadIdx.x;
-    bool defer = false;
     unsigned idx = 0;
-    if (i < nw) {
-      idx = W[i];
-      defer = pass_item<PASS, ND>(a, list, idx);
-    }
+    if (i < nw) idx = W[i];
+    const bool defer = pass_item_local<PASS, ND>(a, list, idx, i < nw);
     const unsigned m = __ballot_sync(0xffffffffu, defer);
     unsigned wb = 0;
     if (lane == 0 && m) wb = atomicAdd(wn_count, (unsigned)__popc(m));
@@ -900,12 +916,9 @@ pass_coop_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(cnts + ((round + 1) % 3), 0u);
     for (unsigned base = blockIdx.x * blockDim.x; base < nw; base += stride) {
       const unsigned i = base + threadIdx.x;
-      bool defer = false;
       unsigned idx = 0;
-      if (i < nw) {
-        idx = W ? __ldcg(W + i) : i;
-        defer = pass_item<PASS, ND>(a, list, idx);
-      }
+      if (i < nw) idx = W ? __ldcg(W + i) : i;
+      const bool defer = pass_item_local<PASS, ND>(a, list, idx, i < nw);
       const unsigned m = __ballot_sync(0xffffffffu, defer);
       unsigned wb = 0;
       if (lane == 0 && m) wb = atomicAdd(cnt, (unsigned)__popc(m));
