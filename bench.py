@@ -469,9 +469,10 @@ def run_reference_arm(args):
         return 0
     f = synth.config3(args.side)
     threads = os.cpu_count() or 1
-    # each step is a bounded sample: about 25 s of CPU work over all steps at
-    # 256 planes per 10 s, never fewer than 16 planes
-    planes = int(min(args.cpu_planes, max(16, 640 // max(1, args.steps))))
+    # each step is a bounded sample of the field: 128 planes (33.5 M elements,
+    # far larger than the host caches, so the rate stands for the whole field)
+    # for up to 20 steps, fewer planes per step for more steps (about 100 s in all)
+    planes = int(min(args.cpu_planes, 128, max(32, 2560 // max(1, args.steps))))
     for _ in range(args.warmup):
         reference_leg(f, 4, threads)
     vals, info = [], None
