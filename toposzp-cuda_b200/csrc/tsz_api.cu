@@ -604,13 +604,12 @@ static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, s
   const bool post = postprocess != 0;
   const bool parse = d_blk_index == nullptr;
   const bool have_sort = d_sort && sort_bytes > 8;
-  size_t need = (post ? a256(n * 4) + post_scratch_bytes(n) + a256(n * 4) : 0) + a256(n) + 8192;
+  size_t need = (post ? post_scratch_bytes(n) + a256(n * 4) : 0) + a256(n) + 8192;
   if (parse)
     need += a256(2 * nb * 8) + parse_scratch_bytes(topo_bytes - 8, B, true) +
             (post && have_sort ? parse_scratch_bytes(sort_bytes - 8, B, false) : 0);
   if (!ctx->scratch.reserve(need)) return -1;
   Arena &A = ctx->scratch;
-  float *O = post ? A.take<float>(n) : nullptr;
   int *sp = post ? A.take<int>(n) : nullptr;
   unsigned char *T = d_types ? d_types : A.take<unsigned char>(n);
   unsigned long long *idx = parse ? A.take<unsigned long long>(2 * nb)
@@ -638,9 +637,6 @@ static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, s
   if (cuda_fail(launch_decode(true, a, s), "decode")) return -1;
   ctx->launches += 1;
   tl_mark(ctx, "decode_topo");
-  if (post && cuda_fail(cudaMemcpyAsync(O, d_out, n * 4, cudaMemcpyDeviceToDevice, s), "copy"))
-    return -1;
-  if (post) tl_mark(ctx, "copy_orig");
   if (parse && post && have_sort) {
     // the sort stream holds one value per extremum: its element count is the
     // decoder's count of type-1/2 tags, read on the device
@@ -687,7 +683,9 @@ static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, s
   unsigned *Lb = A.take<unsigned>((n + 31) / 32);
   if (!S || !desc || !Lb) { set_error("scratch arena too small for post-processing"); return -1; }
   int restored = 0;
-  return postprocess_with(ctx, d_out, O, T, S, desc, Lb, spp, spp ? E : 0, g, absErrBound,
+  // d_out holds the raw decoded field: the list build gathers the raw values
+  // of the candidates from it before any pass updates it in place
+  return postprocess_with(ctx, d_out, d_out, T, S, desc, Lb, spp, spp ? E : 0, g, absErrBound,
                           postprocess == 2, &restored);
 }
 

@@ -6,17 +6,23 @@
 // place, so a point sees the FINAL values of earlier points and the
 // PRE-PASS values of later points.  Only a pass's candidates change (extrema
 // for the stencil and enforcement passes, lost saddles for RBF, saddles for
-// the axis-pattern stencil), so the passes run over compact candidate lists:
-//   * F holds the field before the pass and is not written during the pass;
-//   * a candidate's result goes to S[e] = (generation << 32) | float bits;
+// the axis-pattern stencil), so the passes run over compact candidate lists
+// and update F in place as well:
+//   * a candidate's result goes to F[e] and, with the pass's generation, to
+//     S[e] = (generation << 32) | float bits: one 64-bit word that a reader
+//     takes whole (relaxed), so value and readiness never need ordering;
 //   * a candidate is computed once every EARLIER candidate it reads has its
-//     result for this pass (a neighbour read then returns that result; every
-//     other read returns F); otherwise it is deferred to the next round.
+//     result for this pass (read from S); otherwise it is deferred to the
+//     next round;
+//   * every LATER point a candidate reads lists that candidate among its own
+//     earlier reads, so it cannot have been updated yet: F still holds its
+//     pre-pass value, exactly as in the serial pass.
 // Rounds repeat over the deferred items until none is left (their number is
-// the longest chain of adjacent candidates in raster order), and a list
-// scatter then copies the pass results into F.  Floating-point expressions use
-// explicit round-to-nearest intrinsics so that no multiply-add is contracted
-// (the reference host code is compiled without contraction).
+// the longest chain of adjacent candidates in raster order).  The raw decoded
+// value each point is clamped against is gathered per list entry when the
+// lists are built.  Floating-point expressions use explicit round-to-nearest
+// intrinsics so that no multiply-add is contracted (the reference host code is
+// compiled without contraction).
 #include <cfloat>
 
 #include "tsz_lookback.cuh"
@@ -59,25 +65,21 @@ __constant__ double c_w2[9];
 __constant__ double c_w3[27];
 
 struct PostArgs {
-  float *F;
-  const float *O;
-  unsigned char *T;             // types in bits 0..1, candidate flag in bit 7
+  float *F;                     // the field, updated in place
+  const float *OL;              // raw decoded value of each entry of the pass's list
+  unsigned char *T;             // types in bits 0..1
   const int *sp;
   unsigned long long n_sp;
   Geom g;
   long long n;
   float eb;
   float eps;
-  unsigned gen;
-  unsigned long long *S;
+  unsigned gen;                 // generation of the current pass
+  unsigned long long *S;        // (generation << 32) | result bits, per point
   const unsigned *L;            // lock bitmap: interior point next to an interior extremum
   const unsigned *R;            // RBF candidates (lost saddles) bitmap
-  TileDesc *desc;
-  unsigned *tile_ctr;
   int *err;
   unsigned *restored;
-  bool prev_in_S;               // this pass's candidates hold their pre-pass values in S
-                                // (the previous pass ran over the same list, unscattered)
 };
 
 __device__ __forceinline__ unsigned long long ld_rlx(const unsigned long long *p) {
@@ -134,7 +136,7 @@ __device__ __forceinline__ bool interior_off(const PostArgs &a, const C3 &c, int
   return qi;
 }
 
-// result of candidate q for the current pass, or -1 when not available yet
+// candidate q has its result for the current pass
 __device__ __forceinline__ bool result_ready(const PostArgs &a, long long q) {
   return (unsigned)(ld_rlx(&a.S[q]) >> 32) == a.gen;
 }
@@ -194,8 +196,7 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) {
 }
 
 // 2D stencil (example/test_cuda_topology.cu:118-165)
-__device__ float stencil2(const PostArgs &a, long long e, const C3 &c, int t, int s) {
-  const float o = a.O[e];
+__device__ float stencil2(const PostArgs &a, long long e, const C3 &c, int t, int s, float o) {
   const float hi = __fadd_rn(o, a.eb), lo = __fsub_rn(o, a.eb);
   float m = a.F[e];
   const int ofs[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
@@ -212,8 +213,7 @@ __device__ float stencil2(const PostArgs &a, long long e, const C3 &c, int t, in
 }
 
 // 3D stencil (example/test_cuda_topology_3d.cu:77-128)
-__device__ float stencil3(const PostArgs &a, long long e, const C3 &c, int t, int s) {
-  const float o = a.O[e];
+__device__ float stencil3(const PostArgs &a, long long e, const C3 &c, int t, int s, float o) {
   const float d = __fmul_rn(a.eb, 0.999f);
   const float hi = __fadd_rn(o, d), lo = __fsub_rn(o, d);
   const long long pl = a.g.plane, d3 = a.g.d3;
@@ -233,33 +233,24 @@ __device__ float stencil3(const PostArgs &a, long long e, const C3 &c, int t, in
   return clampf(target, lo, hi);
 }
 
-// pre-pass value of the enforcement pass at e + (dx, dy, dz), for e itself and
-// later points: after an unscattered stencil pass a candidate's value is its
-// stencil result in S; every other point still holds its value in F
-__device__ __forceinline__ float pre_value(const PostArgs &a, long long e, const C3 &c, int dx, int dy, int dz) {
-  const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
-  if (a.prev_in_S && is_cand_known<kPassEnforce>(a, q, interior_off(a, c, dx, dy, dz)))
-    return __uint_as_float((unsigned)ld_rlx(&a.S[q]));
-  return a.F[q];
-}
-
 // enforcement (example/test_cuda_topology.cu:168-198, _3d.cu:131-167)
 template <int ND>
-__device__ float enforce(const PostArgs &a, long long e, const C3 &c, int t) {
-  const float o = a.O[e];
+__device__ float enforce(const PostArgs &a, long long e, const C3 &c, int t, float o) {
   const float d = __fmul_rn(a.eb, 0.999f);
   const float hi = __fadd_rn(o, d), lo = __fsub_rn(o, d);
   const float soft = __fmul_rn(0.25f, a.eps);
-  const float cur = pre_value(a, e, c, 0, 0, 0);
+  const float cur = a.F[e];
   float m;
   if (ND == 2) {
-    const float n = valo<kPassEnforce>(a, e, c, 0, -1, 0), s = pre_value(a, e, c, 0, 1, 0);
-    const float w = valo<kPassEnforce>(a, e, c, 0, 0, -1), ea = pre_value(a, e, c, 0, 0, 1);
+    const long long cols = a.g.d3;
+    const float n = valo<kPassEnforce>(a, e, c, 0, -1, 0), s = a.F[e + cols];
+    const float w = valo<kPassEnforce>(a, e, c, 0, 0, -1), ea = a.F[e + 1];
     m = (t == 1) ? fmaxf(fmaxf(n, s), fmaxf(w, ea)) : fminf(fminf(n, s), fminf(w, ea));
   } else {
-    const float xm = valo<kPassEnforce>(a, e, c, -1, 0, 0), xp = pre_value(a, e, c, 1, 0, 0);
-    const float ym = valo<kPassEnforce>(a, e, c, 0, -1, 0), yp = pre_value(a, e, c, 0, 1, 0);
-    const float zm = valo<kPassEnforce>(a, e, c, 0, 0, -1), zp = pre_value(a, e, c, 0, 0, 1);
+    const long long pl = a.g.plane, d3 = a.g.d3;
+    const float xm = valo<kPassEnforce>(a, e, c, -1, 0, 0), xp = a.F[e + pl];
+    const float ym = valo<kPassEnforce>(a, e, c, 0, -1, 0), yp = a.F[e + d3];
+    const float zm = valo<kPassEnforce>(a, e, c, 0, 0, -1), zp = a.F[e + 1];
     m = (t == 1) ? fmaxf(fmaxf(xm, xp), fmaxf(fmaxf(ym, yp), fmaxf(zm, zp)))
                  : fminf(fminf(xm, xp), fminf(fminf(ym, yp), fminf(zm, zp)));
   }
@@ -288,7 +279,7 @@ __device__ __forceinline__ int cls4_eps(float c, float n, float s, float w, floa
 }
 
 // 2D RBF saddle restoration of candidate e (example/test_cuda_topology.cu:227-326)
-__device__ float rbf2(const PostArgs &a, long long e, const C3 &c, bool &ok) {
+__device__ float rbf2(const PostArgs &a, long long e, const C3 &c, float o, bool &ok) {
   const long long cols = a.g.d3;
   const long long rows = a.g.d2;
   ok = false;
@@ -307,7 +298,6 @@ __device__ float rbf2(const PostArgs &a, long long e, const C3 &c, bool &ok) {
     }
   const float old = a.F[e];
   if (!(den > 0.0)) return old;
-  const float o = a.O[e];
   const float d = __fmul_rn(a.eb, 0.999f);
   const float lo = __fsub_rn(o, d), hi = __fadd_rn(o, d);
   const float n = v[0][1], s = v[2][1], w = v[1][0], ea = v[1][2];
@@ -402,7 +392,7 @@ __device__ bool valid3(const PostArgs &a, long long e, const C3 &c, Win3 &W, flo
 // the 3x3x3 box around e and the points two steps out along each axis, the
 // latter only where the serial code would read them (the neighbour on that
 // side is interior and regular).  A trial changes only the centre value.
-__device__ float rbf3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
+__device__ float rbf3(const PostArgs &a, long long e, const C3 &c, float o, bool &ok) {
   ok = false;
   const float old = a.F[e];
   float v[27];   // box value at (dx, dy, dz): v[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)]
@@ -417,7 +407,6 @@ __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
     den = __dadd_rn(den, ww);
   }
   if (!(den > 0.0)) return old;
-  const float o = a.O[e];
   const float d = __fmul_rn(a.eb, 0.999f);
   const float lo = __fsub_rn(o, d), hi = __fadd_rn(o, d);
   float cand = __double2float_rn(__ddiv_rn(num, den));
@@ -463,14 +452,13 @@ __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
 }
 
 // 3D axis-pattern saddle stencil (example/test_cuda_topology_3d.cu:187-314)
-__device__ float axis3(const PostArgs &a, long long e, const C3 &c, bool &ok) {
+__device__ float axis3(const PostArgs &a, long long e, const C3 &c, float o, bool &ok) {
   ok = false;
   Win3 W;
   W.c = c;
   for (int i = 0; i < 125; i++) (&W.have[0][0][0])[i] = 0;
   const float old = a.F[e];
   if (cls6_at<kPassAxis>(a, e, W, 0, 0, 0, old) == 3) return old;
-  const float o = a.O[e];
   const float d = __fmul_rn(a.eb, 0.999f);
   const float lo = __fsub_rn(o, d), hi = __fadd_rn(o, d);
   const float nb[6] = {w3getp<kPassAxis>(a, e, W, -1, 0, 0, old), w3getp<kPassAxis>(a, e, W, 1, 0, 0, old),
@@ -607,14 +595,15 @@ list_write_kernel(const unsigned char *__restrict__ T, Geom g, long long n, cons
 // their entries through shared memory so each tile's slice of X and Z is
 // stored contiguously (X staged from the front of one buffer, Z from its back:
 // a point is in at most one list).  The last tile writes the totals to
-// tot[0] = (extrema << 32) | saddles.
+// tot[0] = (extrema << 32) | saddles.  The raw decoded value of every list
+// entry (O at its point) goes to OX / OZ beside it.
 constexpr int kListPer = 32;
 constexpr int kListTile = kPostThreads * kListPer;
 
 __global__ void __launch_bounds__(kPostThreads)
 list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, TileDesc *desc, unsigned *tile_ctr,
                   int *err, unsigned *X, unsigned *Z, unsigned char *Eb, unsigned char *Ib,
-                  unsigned long long *tot) {
+                  unsigned long long *tot, const float *__restrict__ O, float *OX, float *OZ) {
   __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
   __shared__ unsigned s_buf[kListTile];
   __shared__ long long s_tile;
@@ -704,8 +693,16 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
     }
     __syncthreads();
     const unsigned long long xb = s_xb, zb = s_zb;
-    for (unsigned k = threadIdx.x; k < te; k += kPostThreads) X[xb + k] = s_buf[k];
-    for (unsigned k = threadIdx.x; k < ts; k += kPostThreads) Z[zb + k] = s_buf[kListTile - 1 - k];
+    for (unsigned k = threadIdx.x; k < te; k += kPostThreads) {
+      const unsigned q = s_buf[k];
+      X[xb + k] = q;
+      OX[xb + k] = O[q];
+    }
+    for (unsigned k = threadIdx.x; k < ts; k += kPostThreads) {
+      const unsigned q = s_buf[kListTile - 1 - k];
+      Z[zb + k] = q;
+      OZ[zb + k] = O[q];
+    }
     __syncthreads();
   }
 }
@@ -739,20 +736,24 @@ __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__r
   const long long e = (long long)list[idx];
   const C3 c = coords(a.g, e);
   if (!deps_ready<PASS, ND>(a, e, c)) return true;
+  const float o = a.OL[idx];
   float r;
   bool ok = false;
   if (PASS == kPassStencil) {
     const int t = ty(a, e);
     const int s = (idx < a.n_sp) ? a.sp[idx] : 0;
-    r = (ND == 2) ? stencil2(a, e, c, t, s) : stencil3(a, e, c, t, s);
+    r = (ND == 2) ? stencil2(a, e, c, t, s, o) : stencil3(a, e, c, t, s, o);
   } else if (PASS == kPassEnforce) {
-    r = enforce<ND>(a, e, c, ty(a, e));
+    r = enforce<ND>(a, e, c, ty(a, e), o);
   } else if (PASS == kPassRbf) {
-    r = (ND == 2) ? rbf2(a, e, c, ok) : rbf3(a, e, c, ok);
+    r = (ND == 2) ? rbf2(a, e, c, o, ok) : rbf3(a, e, c, o, ok);
   } else {
-    r = axis3(a, e, c, ok);
+    r = axis3(a, e, c, o, ok);
   }
   if (ok) atomicAdd(a.restored, 1u);
+  // in place: every reader of e's pre-pass value has finished (they are the
+  // earlier candidates e waited for); later readers take e's result from S
+  a.F[e] = r;
   st_rlx(&a.S[e], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
   return false;
 }
@@ -797,15 +798,6 @@ pass_round_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned 
   if (defer) Wn[base + __popc(m & ((1u << lane) - 1u))] = idx;
 }
 
-// F[list[i]] = result of the pass
-__global__ void list_scatter_kernel(float *__restrict__ F, const unsigned long long *__restrict__ S,
-                                    const unsigned *__restrict__ list, unsigned nlist,
-                                    const unsigned *__restrict__ sel) {
-  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nlist) return;
-  const long long e = (long long)list[sel ? sel[i] : i];
-  F[e] = __uint_as_float((unsigned)S[e]);
-}
 
 // A round over a worklist whose length is on the device (*nw_dev), in a
 // grid-stride loop over a grid of any size (no barrier inside).
@@ -877,16 +869,14 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
   return s_ok != 0;
 }
 
-// The rounds of a pass after round 0 (or all of them), and the scatter of the
-// results into F, in one cooperative launch: rounds are separated by grid
-// barriers instead of host round trips.  The worklist starts as W_start with
+// The rounds of a pass after round 1 (or all of them) in one cooperative
+// launch: rounds are separated by grid barriers instead of host round trips.  The worklist starts as W_start with
 // *nstart_dev items (the deferred items of a round-0 launch) or, when W_start
 // is null, as sel (list indices; null = the whole list) with the pass's total
 // item count.  The total is *total_dev when that is not null, else total.
 // Worklists and counters written during the launch are read through L2
 // (__ldcg), since other SMs wrote them.  Every CTA takes the same branch at
-// every barrier: the counts it reads are final after the barrier.  With
-// scatter != 0 the results are copied into F at the end.
+// every barrier: the counts it reads are final after the barrier.
 // status: 0 done, 1 round limit, 2 no progress.
 constexpr int kCoopRoundLimit = 100000;
 
@@ -894,7 +884,7 @@ template <int PASS, int ND>
 __global__ void __launch_bounds__(kPostThreads)
 pass_coop_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *sel, unsigned total,
                  const unsigned *total_dev, const unsigned *W_start, const unsigned *nstart_dev, unsigned *Wx,
-                 unsigned *Wy, unsigned *cnts, unsigned *bar, unsigned long long *status, int scatter) {
+                 unsigned *Wy, unsigned *cnts, unsigned *bar, unsigned long long *status) {
   const unsigned tot = total_dev ? __ldcg(total_dev) : total;
   const unsigned *W = W_start ? W_start : sel;
   unsigned nw = W_start ? __ldcg(nstart_dev) : tot;
@@ -935,11 +925,7 @@ pass_coop_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *
     nw = next;
     b ^= 1;
   }
-  if (!scatter) return;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += stride) {
-    const long long e = (long long)list[sel ? __ldcg(sel + i) : i];
-    a.F[e] = __uint_as_float((unsigned)ld_rlx(&a.S[e]));
-  }
+  (void)tot;
 }
 
 // bits [b, b + 32) of a bitmap of nbits bits (zeros outside)
@@ -1003,9 +989,11 @@ static cudaError_t upload_weights(int dev) {
 size_t post_scratch_bytes(unsigned long long n) {
   const unsigned long long ntiles = (n + kPostTile - 1) / kPostTile;
   const unsigned long long words = (n + 31) / 32;
-  // T, descriptors, lock + RBF bitmaps, lists X and Z, worklists (2), Y
-  return a256(n) + a256((ntiles + 1) * sizeof(TileDesc)) + 4 * a256(words * 4 + 4) + 5 * a256(n * 4) + 8192;
+  // T, descriptors, lock + RBF + extrema + interior bitmaps, lists X and Z,
+  // worklists (2), Y, raw values of X and Z
+  return a256(n) + a256((ntiles + 1) * sizeof(TileDesc)) + 4 * a256(words * 4 + 4) + 7 * a256(n * 4) + 8192;
 }
+
 
 // generation counter of the result words (never reused while the buffer lives)
 static unsigned next_gen(szp_b200_ctx *ctx) { return ++ctx->post_gen; }
@@ -1035,7 +1023,7 @@ unsigned long long *post_words(szp_b200_ctx *ctx, unsigned long long n) {
 // the host-driven rounds).
 template <int PASS, int ND>
 static int run_pass_coop(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, const unsigned *sel,
-                         unsigned count, const unsigned *count_dev, unsigned *W0, unsigned *W1, int scatter = 1) {
+                         unsigned count, const unsigned *count_dev, unsigned *W0, unsigned *W1) {
   static int grid_for_dev[64];
   const int dev = ctx->device;
   if (dev < 0 || dev >= 64) return 1;
@@ -1081,7 +1069,7 @@ static int run_pass_coop(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, c
   }
   void *args[] = {(void *)&a,   (void *)&list,   (void *)&sel, (void *)&count, (void *)&count_dev,
                   (void *)&W_start, (void *)&nstart, (void *)&Wx, (void *)&Wy, (void *)&cnts,
-                  (void *)&bar, (void *)&status, (void *)&scatter};
+                  (void *)&bar, (void *)&status};
   if (cuda_fail(cudaLaunchCooperativeKernel((const void *)pass_coop_kernel<PASS, ND>, dim3(grid_for_dev[dev]),
                                             dim3(kPostThreads), args, 0, s),
                 "cooperative pass launch"))
@@ -1116,11 +1104,7 @@ static int run_rounds(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, unsi
     nw = next;
     b ^= 1;
   }
-  if (count) {
-    list_scatter_kernel<<<(count + 255) / 256, 256, 0, s>>>(a.F, a.S, list, count, sel_for_scatter);
-    ctx->launches += 1;
-    if (cuda_fail(cudaGetLastError(), "scatter")) return -1;
-  }
+  (void)sel_for_scatter;
   return 0;
 }
 
@@ -1151,34 +1135,28 @@ static int run_rounds_sel(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, 
     nw = next;
     b ^= 1;
   }
-  list_scatter_kernel<<<(count + 255) / 256, 256, 0, s>>>(a.F, a.S, list, count, sel);
-  ctx->launches += 1;
-  return cuda_fail(cudaGetLastError(), "scatter") ? -1 : 0;
+  return 0;
 }
 
 template <int ND>
 static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned nx, unsigned *Z, unsigned nz,
                           unsigned *Y, unsigned *W0, unsigned *W1, unsigned *R, unsigned *Lb,
-                          const unsigned *Eb, const unsigned *Ib, int axis_stencil) {
+                          const unsigned *Eb, const unsigned *Ib, const float *OX, const float *OZ,
+                          int axis_stencil) {
   cudaStream_t s = ctx->stream;
   const long long n = a.n;
-  a.prev_in_S = false;
+  a.OL = OX;
   if (a.sp && a.n_sp > 0) {
-    // the stencil results stay in S: enforcement runs over the same list and
-    // reads its candidates' pre-pass values there, so F is written once
     a.gen = next_gen(ctx);
-    const int rc = run_pass_coop<kPassStencil, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1, 0);
-    if (rc < 0) return -1;
-    if (rc > 0 && run_rounds<kPassStencil, ND>(ctx, a, X, nx, W0, W1, nullptr)) return -1;
-    a.prev_in_S = rc == 0;
+    const int rc = run_pass_coop<kPassStencil, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
+    if (rc < 0 || (rc > 0 && run_rounds<kPassStencil, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
     tl_mark(ctx, "post_stencil");
   }
-  a.gen = next_gen(ctx);
   {
+    a.gen = next_gen(ctx);
     const int rc = run_pass_coop<kPassEnforce, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
     if (rc < 0 || (rc > 0 && run_rounds<kPassEnforce, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
   }
-  a.prev_in_S = false;
   tl_mark(ctx, "post_enforce");
   // locks (static: from the types) and the lost saddles (from F after enforcement)
   const long long words = (n + 31) / 32;
@@ -1194,6 +1172,7 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   tl_mark(ctx, "post_fn_locks");
   // RBF runs over Z restricted to the lost saddles (Y holds indices into Z);
   // their number stays on the device
+  a.OL = OZ;
   a.gen = next_gen(ctx);
   const int rc = nz ? run_pass_coop<kPassRbf, ND>(ctx, a, Z, Y, 0, ycnt, W0, W1) : 0;
   if (rc < 0) return -1;
@@ -1216,8 +1195,7 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
 
 int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsigned char *d_T,
                      unsigned long long *d_S, TileDesc *desc, unsigned *d_L, const int *d_sp,
-                     unsigned long long n_sp, const Geom &g, float eb, int axis_stencil,
-                     int *restored_out) {
+                     unsigned long long n_sp, const Geom &g, float eb, int axis_stencil, int *restored_out) {
   const long long n = g.d1 * g.d2 * g.d3;
   if (g.d2 < 3 || g.d3 < 3 || (g.nd == 3 && g.d1 < 3)) { if (restored_out) *restored_out = 0; return 0; }
   if (n >= (1ll << 32)) { set_error("post-processing supports fields of fewer than 2^32 points"); return -1; }
@@ -1230,7 +1208,8 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   unsigned *W0 = A.take<unsigned>(n), *W1 = A.take<unsigned>(n);
   unsigned *R = A.take<unsigned>((n + 31) / 32);
   unsigned *Eb = A.take<unsigned>((n + 31) / 32 + 1), *Ib = A.take<unsigned>((n + 31) / 32 + 1);
-  if (!X || !Z || !Y || !W0 || !W1 || !R || !Eb || !Ib) {
+  float *OX = A.take<float>(n), *OZ = A.take<float>(n);
+  if (!X || !Z || !Y || !W0 || !W1 || !R || !Eb || !Ib || !OX || !OZ) {
     set_error("scratch arena too small for post-processing");
     return -1;
   }
@@ -1252,7 +1231,7 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
     const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 4);
     list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
                                                     Z, reinterpret_cast<unsigned char *>(Eb),
-                                                    reinterpret_cast<unsigned char *>(Ib), d_tot);
+                                                    reinterpret_cast<unsigned char *>(Ib), d_tot, d_orig, OX, OZ);
   }
   ctx->launches += 1;
   unsigned long long tot = 0;
@@ -1264,7 +1243,6 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   tl_mark(ctx, "post_lists");
   PostArgs a{};
   a.F = d_data;
-  a.O = d_orig;
   a.T = d_T;
   a.sp = d_sp;
   a.n_sp = d_sp ? n_sp : 0;
@@ -1273,11 +1251,11 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   a.eb = eb;
   a.eps = fmaxf(1e-6f, 0.1f * eb);
   a.S = d_S;
-  a.desc = desc;
   a.err = reinterpret_cast<int *>(w + 4);
   a.restored = reinterpret_cast<unsigned *>(w + 5);
-  const int rc = (g.nd == 2) ? run_all_passes<2>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, axis_stencil)
-                             : run_all_passes<3>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, axis_stencil);
+  const int rc = (g.nd == 2)
+                     ? run_all_passes<2>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, OX, OZ, axis_stencil)
+                     : run_all_passes<3>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, OX, OZ, axis_stencil);
   if (rc) return -1;
   if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 96, cudaMemcpyDeviceToHost, s), "D2H") ||
       cuda_fail(cudaStreamSynchronize(s), "postprocess"))

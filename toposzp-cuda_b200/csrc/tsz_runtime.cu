@@ -89,9 +89,9 @@ static void ctx_free(szp_b200_ctx *c) {
   for (int i = 0; i <= szp_b200_ctx::kMaxStages; i++)
     if (c->ev[i]) { cudaEventDestroy(c->ev[i]); c->ev[i] = nullptr; }
   c->scratch.release();
-  c->io.release();
   if (c->post_S) cudaFree(c->post_S);
   c->post_S = nullptr;
+  c->io.release();
   if (c->h_words) cudaFreeHost(c->h_words);
   if (c->d_words) cudaFree(c->d_words);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
