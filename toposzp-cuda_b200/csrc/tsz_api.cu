@@ -533,11 +533,16 @@ static bool geom_ok(const szp_b200_geom &g, unsigned long long *n, Geom *out) {
 
 extern "C" {
 
-int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_data, szp_b200_geom geom,
-                               float absErrBound, int blockSize, unsigned char *d_topo,
-                               unsigned char *d_sort, uint64_t *d_blk_index,
-                               szp_b200_sizes *sizes) {
-  clear_error();
+}  // extern "C"
+
+namespace tsz {
+
+// Fused compression.  With h_topo set, the topology stream is copied to the
+// host on the workspace's copy stream as soon as it is complete, overlapping
+// the rank and sort-position stages (the caller waits for the copy stream).
+static int compress_dev_impl(szp_b200_ctx *ctx, const float *d_data, szp_b200_geom geom, float absErrBound,
+                             int blockSize, unsigned char *d_topo, unsigned char *d_sort, uint64_t *d_blk_index,
+                             szp_b200_sizes *sizes, unsigned char *h_topo, size_t topo_cap) {
   if (!ctx || !d_data || !d_topo || !d_sort || !sizes) { set_error("null argument"); return -1; }
   if (!(absErrBound > 0.0f)) { set_error("error bound must be positive"); return -1; }
   if (!check_block_size(blockSize, "szp_b200_topo_compress_dev")) return -1;
@@ -564,6 +569,16 @@ int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_data, szp_b200_
   sizes->cp_count = tot[1];
   sizes->extrema_count = tot[2];
   sizes->sort_bytes = 0;
+  if (h_topo) {
+    // the encoder has finished (encode_pass waited for it): copy now
+    if (sizes->topo_bytes > topo_cap) {
+      set_error("topology output buffer too small (%zu bytes needed)", sizes->topo_bytes);
+      return -1;
+    }
+    cudaStream_t cs = copy_stream(ctx);
+    if (!cs || cuda_fail(cudaMemcpyAsync(h_topo, d_topo, sizes->topo_bytes, cudaMemcpyDeviceToHost, cs), "D2H"))
+      return -1;
+  }
   const unsigned long long K = tot[1], E = tot[2];
   if (E == 0) return 0;
   if (rank_positions(ctx, pairs, nullptr, K, E, absErrBound, sp)) return -1;
@@ -579,6 +594,19 @@ int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_data, szp_b200_
   return 0;
 }
 
+}  // namespace tsz
+
+extern "C" {
+
+int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_data, szp_b200_geom geom,
+                               float absErrBound, int blockSize, unsigned char *d_topo,
+                               unsigned char *d_sort, uint64_t *d_blk_index,
+                               szp_b200_sizes *sizes) {
+  clear_error();
+  return compress_dev_impl(ctx, d_data, geom, absErrBound, blockSize, d_topo, d_sort, d_blk_index, sizes, nullptr,
+                           0);
+}
+
 }  // extern "C"
 
 namespace tsz {
@@ -591,7 +619,7 @@ static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, s
                                const unsigned char *d_sort, size_t sort_bytes,
                                const uint64_t *d_blk_index, szp_b200_geom geom, float absErrBound,
                                int blockSize, float *d_out, unsigned char *d_types, int postprocess,
-                               bool ref_bound, bool *parse_failed) {
+                               bool ref_bound, bool *parse_failed, cudaEvent_t sort_ready = nullptr) {
   if (parse_failed) *parse_failed = false;
   if (!ctx || !d_topo || !d_out) { set_error("null argument"); return -1; }
   if (!check_block_size(blockSize, "szp_b200_topo_decompress_dev")) return -1;
@@ -637,6 +665,8 @@ static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, s
   if (cuda_fail(launch_decode(true, a, s), "decode")) return -1;
   ctx->launches += 1;
   tl_mark(ctx, "decode_topo");
+  // the sort stream may still be on its way to the device (host-buffer path)
+  if (sort_ready && post && have_sort && cuda_fail(cudaStreamWaitEvent(s, sort_ready, 0), "wait")) return -1;
   if (parse && post && have_sort) {
     // the sort stream holds one value per extremum: its element count is the
     // decoder's count of type-1/2 tags, read on the device
@@ -809,17 +839,22 @@ int szp_b200_topo_compress_host(szp_b200_ctx *ctx, const float *h_data, szp_b200
   cudaStream_t s = ctx->stream;
   if (cuda_fail(cudaMemcpyAsync(d_data, h_data, n * 4, cudaMemcpyHostToDevice, s), "H2D field"))
     return -1;
-  if (szp_b200_topo_compress_dev(ctx, d_data, geom, absErrBound, blockSize, d_topo, d_sort, nullptr,
-                                 sizes))
-    return -1;
-  if (sizes->topo_bytes > topo_cap || sizes->sort_bytes > sort_cap) {
-    set_error("output buffers too small (%zu / %zu bytes needed)", sizes->topo_bytes, sizes->sort_bytes);
+  // the topology stream goes to the host while the rank and sort stages run
+  const int rc = compress_dev_impl(ctx, d_data, geom, absErrBound, blockSize, d_topo, d_sort, nullptr, sizes,
+                                   h_topo, topo_cap);
+  cudaStream_t cs = ctx->copy_stream;
+  if (rc) {
+    if (cs) cudaStreamSynchronize(cs);
     return -1;
   }
-  if (cuda_fail(cudaMemcpyAsync(h_topo, d_topo, sizes->topo_bytes, cudaMemcpyDeviceToHost, s), "D2H") ||
-      (sizes->sort_bytes &&
+  if (sizes->sort_bytes > sort_cap) {
+    if (cs) cudaStreamSynchronize(cs);
+    set_error("sort-position output buffer too small (%zu bytes needed)", sizes->sort_bytes);
+    return -1;
+  }
+  if ((sizes->sort_bytes &&
        cuda_fail(cudaMemcpyAsync(h_sort, d_sort, sizes->sort_bytes, cudaMemcpyDeviceToHost, s), "D2H")) ||
-      cuda_fail(cudaStreamSynchronize(s), "sync"))
+      cuda_fail(cudaStreamSynchronize(s), "sync") || (cs && cuda_fail(cudaStreamSynchronize(cs), "sync")))
     return -1;
   return 0;
 }
@@ -919,12 +954,20 @@ int szp_b200_topo_decompress_host(szp_b200_ctx *ctx, const unsigned char *h_topo
     unsigned char *d_sort = ctx->io.take<unsigned char>(sbytes + 16);
     float *d_out = ctx->io.take<float>(n);
     cudaStream_t s = ctx->stream;
+    // the sort stream travels on the copy stream while the topology stream is
+    // parsed and decoded
+    cudaStream_t cs = sbytes ? copy_stream(ctx) : nullptr;
+    if (sbytes && !cs) return -1;
     if (cuda_fail(cudaMemcpyAsync(d_topo, h_topo, topo_bytes, cudaMemcpyHostToDevice, s), "H2D") ||
-        (sbytes && cuda_fail(cudaMemcpyAsync(d_sort, h_sort, sbytes, cudaMemcpyHostToDevice, s), "H2D")))
+        (sbytes && (cuda_fail(cudaMemcpyAsync(d_sort, h_sort, sbytes, cudaMemcpyHostToDevice, cs), "H2D") ||
+                    cuda_fail(cudaEventRecord(ctx->copy_ev, cs), "event"))))
       return -1;
     bool parse_failed = false;
-    if (decompress_dev_impl(ctx, d_topo, topo_bytes, sbytes ? d_sort : nullptr, sbytes, nullptr, geom,
-                            absErrBound, blockSize, d_out, nullptr, postprocess, true, &parse_failed) == 0) {
+    const int rc = decompress_dev_impl(ctx, d_topo, topo_bytes, sbytes ? d_sort : nullptr, sbytes, nullptr, geom,
+                                       absErrBound, blockSize, d_out, nullptr, postprocess, true, &parse_failed,
+                                       sbytes ? ctx->copy_ev : nullptr);
+    if (cs) cudaStreamSynchronize(cs);
+    if (rc == 0) {
       if (cuda_fail(cudaMemcpyAsync(h_out, d_out, n * 4, cudaMemcpyDeviceToHost, s), "D2H") ||
           cuda_fail(cudaStreamSynchronize(s), "sync"))
         return -1;

@@ -84,8 +84,25 @@ void tl_mark(szp_b200_ctx *ctx, const char *name) {
   ctx->nstage++;
 }
 
+cudaStream_t copy_stream(szp_b200_ctx *ctx) {
+  if (!ctx->copy_stream) {
+    if (cuda_fail(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate"))
+      return nullptr;
+    if (cuda_fail(cudaEventCreateWithFlags(&ctx->copy_ev, cudaEventDisableTiming), "cudaEventCreate")) {
+      cudaStreamDestroy(ctx->copy_stream);
+      ctx->copy_stream = nullptr;
+      return nullptr;
+    }
+  }
+  return ctx->copy_stream;
+}
+
 static void ctx_free(szp_b200_ctx *c) {
   if (!c) return;
+  if (c->copy_stream) { cudaStreamSynchronize(c->copy_stream); cudaStreamDestroy(c->copy_stream); }
+  if (c->copy_ev) cudaEventDestroy(c->copy_ev);
+  c->copy_stream = nullptr;
+  c->copy_ev = nullptr;
   for (int i = 0; i <= szp_b200_ctx::kMaxStages; i++)
     if (c->ev[i]) { cudaEventDestroy(c->ev[i]); c->ev[i] = nullptr; }
   c->scratch.release();

@@ -51,6 +51,9 @@ struct szp_b200_ctx {
   int nstage = 0;
   bool timeline_started = false;
   unsigned long long launches = 0;         // kernels launched through this workspace
+  // second stream for host copies that overlap work on `stream` (created on first use)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ev = nullptr;
 };
 
 namespace tsz {
@@ -62,6 +65,9 @@ szp_b200_ctx *default_ctx();
 // each stage's work has been enqueued on ctx->stream.
 void tl_begin(szp_b200_ctx *ctx);
 void tl_mark(szp_b200_ctx *ctx, const char *name);
+
+// The workspace's copy stream and its event (created on first use); null on failure.
+cudaStream_t copy_stream(szp_b200_ctx *ctx);
 
 // Rounds a byte count up to 256.
 inline size_t a256(size_t b) { return (b + 255) & ~(size_t)255; }
