@@ -283,3 +283,26 @@ def test_host_decompress_two_chunk_table(T, ora):
                         len(s_sp), dims, eb, B, out, 1)
     assert (bits(out) == bits(ref)).all()
     ctx.close()
+
+
+def test_host_compress_in_parts_matches_device(T):
+    """From 2^24 elements the host-buffer compressor copies the field in parts
+    that overlap the encoder; its streams equal the device-resident call's."""
+    import torch
+    dims = (256, 256, 256)
+    d = synth.small_field(dims, seed=12, kind="band")
+    eb, B = 1e-4, 64
+    ctx = T.Context()
+    dd = torch.from_numpy(d.reshape(-1).copy()).cuda()
+    topo, sort, _, sz = ctx.compress(dd, dims, eb, B, index=False)
+    L = T.lib()
+    n = d.size
+    h_topo = torch.empty(L.szp_b200_topo_bound(n, B), dtype=torch.uint8).pin_memory().numpy()
+    h_sort = torch.empty(L.szp_b200_sort_bound(n, B), dtype=torch.uint8).pin_memory().numpy()
+    hf = torch.from_numpy(d).pin_memory().numpy()
+    hz = ctx.compress_host(hf, eb, B, h_topo, h_sort)
+    assert (hz.topo_bytes, hz.sort_bytes, hz.cp_count, hz.extrema_count) == \
+        (sz.topo_bytes, sz.sort_bytes, sz.cp_count, sz.extrema_count)
+    assert h_topo[: hz.topo_bytes].tobytes() == topo[: sz.topo_bytes].cpu().numpy().tobytes()
+    assert h_sort[: hz.sort_bytes].tobytes() == sort[: sz.sort_bytes].cpu().numpy().tobytes()
+    ctx.close()

@@ -106,6 +106,89 @@ int encode_pass(szp_b200_ctx *ctx, int mode, const float *d_data, const int *d_i
   return 0;
 }
 
+// Topology encode of a field that is still on its way from the host: the copy
+// runs in parts on the copy stream and the encoder runs one launch per part,
+// over the tiles whose reads (the tile, and one plane -- one row in 2D --
+// beyond it) the copied data already covers.  Tiles leave the launches in
+// order, so the look-back of a launch only meets completed tiles of earlier
+// launches.  Same results as one encode_pass over the whole field.
+static int encode_topo_chunked(szp_b200_ctx *ctx, const float *h_src, float *d_data, unsigned long long n, int B,
+                               float eb, const Geom &g, unsigned char *d_stream, unsigned long long stream_cap,
+                               unsigned long long *d_blk_off, void *d_cp, unsigned long long cp_cap,
+                               unsigned long long totals_out[3]) {
+  cudaStream_t s = ctx->stream;
+  cudaStream_t cs = copy_stream(ctx);
+  if (!cs) return -1;
+  const int K = 8;
+  const unsigned long long nb = (n + B - 1) / B;
+  const unsigned long long TB = (unsigned long long)enc_tile_blocks(B);
+  const unsigned long long TE = TB * (unsigned long long)B;   // elements per tile
+  const unsigned long long ntiles = (nb + TB - 1) / TB;
+  const unsigned long long halo = (g.nd == 3 ? (unsigned long long)g.plane : (unsigned long long)g.d3) + 1;
+  unsigned long long cut[K + 1];
+  cut[0] = 0;
+  for (int k = 1; k < K; k++) cut[k] = std::min<unsigned long long>(n, (n / K * k) / TE * TE);
+  cut[K] = n;
+  for (int k = 0; k < K; k++) {
+    if (!ctx->chunk_ev[k] && cuda_fail(cudaEventCreateWithFlags(&ctx->chunk_ev[k], cudaEventDisableTiming), "event"))
+      return -1;
+    if (cut[k + 1] > cut[k] &&
+        cuda_fail(cudaMemcpyAsync(d_data + cut[k], h_src + cut[k], (cut[k + 1] - cut[k]) * 4, cudaMemcpyHostToDevice,
+                                  cs), "H2D field"))
+      return -1;
+    if (cuda_fail(cudaEventRecord(ctx->chunk_ev[k], cs), "event")) return -1;
+  }
+  TileDesc *desc = ctx->scratch.take<TileDesc>(ntiles + 1);
+  if (!desc) { set_error("scratch arena too small for tile descriptors"); return -1; }
+  unsigned long long *w = ctx->d_words;  // [0..2] totals, [3] tile counter, [4] err
+  if (cuda_fail(cudaMemsetAsync(desc, 0, (ntiles + 1) * sizeof(TileDesc), s), "memset") ||
+      cuda_fail(cudaMemsetAsync(w, 0, 8 * sizeof(unsigned long long), s), "memset") ||
+      cuda_fail(cudaMemsetAsync(d_stream, 0, 8, s), "memset"))
+    return -1;
+  EncArgs a{};
+  a.data = d_data;
+  a.n = n;
+  a.B = B;
+  a.eb = eb;
+  a.inv = 1.0 / (double)eb;
+  a.g = g;
+  a.out = d_stream + 8;
+  a.out_cap = stream_cap > 8 ? stream_cap - 8 : 0;
+  a.blk_off = d_blk_off;
+  a.tile_ctr = reinterpret_cast<unsigned *>(w + 3);
+  a.err = reinterpret_cast<int *>(w + 4);
+  a.total = w;
+  a.desc = desc;
+  a.cp_mode = kCpPairs;
+  a.cp_out = d_cp;
+  a.cp_cap = cp_cap;
+  unsigned long long done = 0;
+  for (int k = 0; k < K; k++) {
+    if (cuda_fail(cudaStreamWaitEvent(s, ctx->chunk_ev[k], 0), "wait")) return -1;
+    // tiles whose reads end inside [0, cut[k+1])
+    unsigned long long upto = ntiles;
+    if (k < K - 1) upto = cut[k + 1] > halo ? std::min<unsigned long long>(ntiles, (cut[k + 1] - halo) / TE) : 0;
+    if (upto <= done) continue;
+    a.tile_lo = done;
+    a.tile_hi = upto;
+    if (cuda_fail(cudaMemsetAsync(w + 3, 0, 8, s), "memset")) return -1;
+    const int grid = (int)std::min<unsigned long long>(upto - done, (unsigned long long)ctx->sm_count * 8ull);
+    if (cuda_fail(launch_encode(kEncClassify, a, s, grid), "encode launch")) return -1;
+    ctx->launches += 1;
+    done = upto;
+  }
+  if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+                "D2H totals") ||
+      cuda_fail(cudaStreamSynchronize(s), "encode"))
+    return -1;
+  const int err = (int)(ctx->h_words[4] & 0xffffffffu);
+  if (err) { set_error("encoder reported status %d", err); return -1; }
+  totals_out[0] = ctx->h_words[0];
+  totals_out[1] = ctx->h_words[1];
+  totals_out[2] = ctx->h_words[2];
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // host-side walk of a foreign stream: the reference's offset-table thread-count
 // detection and block walk (SZp/src/szp_cuda_decompress.cu:233-328, 339-477).
@@ -542,7 +625,8 @@ namespace tsz {
 // the rank and sort-position stages (the caller waits for the copy stream).
 static int compress_dev_impl(szp_b200_ctx *ctx, const float *d_data, szp_b200_geom geom, float absErrBound,
                              int blockSize, unsigned char *d_topo, unsigned char *d_sort, uint64_t *d_blk_index,
-                             szp_b200_sizes *sizes, unsigned char *h_topo, size_t topo_cap) {
+                             szp_b200_sizes *sizes, unsigned char *h_topo, size_t topo_cap,
+                             const float *h_src = nullptr) {
   if (!ctx || !d_data || !d_topo || !d_sort || !sizes) { set_error("null argument"); return -1; }
   if (!(absErrBound > 0.0f)) { set_error("error bound must be positive"); return -1; }
   if (!check_block_size(blockSize, "szp_b200_topo_compress_dev")) return -1;
@@ -560,9 +644,18 @@ static int compress_dev_impl(szp_b200_ctx *ctx, const float *d_data, szp_b200_ge
   int *sp = A.take<int>(n);
   unsigned long long tot[3];
   tl_begin(ctx);
-  if (encode_pass(ctx, kEncClassify, d_data, nullptr, nullptr, n, B, absErrBound, g, d_topo,
-                  stream_bound(n, B, true), reinterpret_cast<unsigned long long *>(d_blk_index),
-                  kCpPairs, pairs, kcap, tot))
+  // a field still on the host (h_src) is copied in parts that overlap the encoder
+  const bool chunked = h_src && B <= 256 && n >= (1ull << 24);
+  if (h_src && !chunked &&
+      cuda_fail(cudaMemcpyAsync(const_cast<float *>(d_data), h_src, n * 4, cudaMemcpyHostToDevice, ctx->stream),
+                "H2D field"))
+    return -1;
+  if (chunked ? encode_topo_chunked(ctx, h_src, const_cast<float *>(d_data), n, B, absErrBound, g, d_topo,
+                                    stream_bound(n, B, true), reinterpret_cast<unsigned long long *>(d_blk_index),
+                                    pairs, kcap, tot)
+              : encode_pass(ctx, kEncClassify, d_data, nullptr, nullptr, n, B, absErrBound, g, d_topo,
+                            stream_bound(n, B, true), reinterpret_cast<unsigned long long *>(d_blk_index),
+                            kCpPairs, pairs, kcap, tot))
     return -1;
   tl_mark(ctx, "encode_topo");
   sizes->topo_bytes = 8 + tot[0];
@@ -837,11 +930,10 @@ int szp_b200_topo_compress_host(szp_b200_ctx *ctx, const float *h_data, szp_b200
   unsigned char *d_topo = ctx->io.take<unsigned char>(tb);
   unsigned char *d_sort = ctx->io.take<unsigned char>(sb);
   cudaStream_t s = ctx->stream;
-  if (cuda_fail(cudaMemcpyAsync(d_data, h_data, n * 4, cudaMemcpyHostToDevice, s), "H2D field"))
-    return -1;
-  // the topology stream goes to the host while the rank and sort stages run
+  // the field is copied in parts that overlap the encoder; the topology
+  // stream goes to the host while the rank and sort stages run
   const int rc = compress_dev_impl(ctx, d_data, geom, absErrBound, blockSize, d_topo, d_sort, nullptr, sizes,
-                                   h_topo, topo_cap);
+                                   h_topo, topo_cap, h_data);
   cudaStream_t cs = ctx->copy_stream;
   if (rc) {
     if (cs) cudaStreamSynchronize(cs);

@@ -21,6 +21,8 @@ struct EncArgs {
   unsigned long long *blk_off;  // per-block payload offsets (optional)
   TileDesc *desc;               // zeroed, one per tile
   unsigned *tile_ctr;           // zeroed
+  unsigned long long tile_lo;   // tiles [tile_lo, tile_hi) of this launch (tile_hi 0: all)
+  unsigned long long tile_hi;
   int *err;                     // status word
   unsigned long long *total;    // [payload bytes, cps, extrema]
   int cp_mode;                  // CpMode (kEncClassify only)

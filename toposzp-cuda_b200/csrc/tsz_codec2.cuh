@@ -474,7 +474,9 @@ __device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long t
   }
 }
 
-// One field: persistent CTAs claim tiles from a.tile_ctr in order.
+// One field: persistent CTAs claim tiles from a.tile_ctr in order (within
+// [a.tile_lo, a.tile_hi) when a.tile_hi is set: a launch per part of the
+// field, earlier tiles complete).
 template <int MODE, int G>
 __global__ void __launch_bounds__(kThreads, (MODE == kEncClassify ? 3 : 4))
 encode2_kernel(EncArgs a) {
@@ -483,10 +485,10 @@ encode2_kernel(EncArgs a) {
   const long long nblocks = ((long long)a.n + a.B - 1) / a.B;
   const long long ntiles = (nblocks + EncShared<G, kWarps>::TB - 1) / EncShared<G, kWarps>::TB;
   while (true) {
-    if (threadIdx.x == 0) sh.tile = (long long)atomicAdd(a.tile_ctr, 1u);
+    if (threadIdx.x == 0) sh.tile = (long long)a.tile_lo + (long long)atomicAdd(a.tile_ctr, 1u);
     __syncthreads();
     const long long tile = sh.tile;
-    if (tile >= ntiles) break;
+    if (tile >= (a.tile_hi ? (long long)a.tile_hi : ntiles)) break;
     encode2_tile<MODE, G, kWarps>(a, tile, smem_dyn, sh);
   }
 }

@@ -103,6 +103,8 @@ static void ctx_free(szp_b200_ctx *c) {
   if (c->copy_ev) cudaEventDestroy(c->copy_ev);
   c->copy_stream = nullptr;
   c->copy_ev = nullptr;
+  for (int i = 0; i < szp_b200_ctx::kChunkEvents; i++)
+    if (c->chunk_ev[i]) { cudaEventDestroy(c->chunk_ev[i]); c->chunk_ev[i] = nullptr; }
   for (int i = 0; i <= szp_b200_ctx::kMaxStages; i++)
     if (c->ev[i]) { cudaEventDestroy(c->ev[i]); c->ev[i] = nullptr; }
   c->scratch.release();

@@ -54,6 +54,8 @@ struct szp_b200_ctx {
   // second stream for host copies that overlap work on `stream` (created on first use)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t copy_ev = nullptr;
+  static constexpr int kChunkEvents = 16;
+  cudaEvent_t chunk_ev[kChunkEvents] = {};   // parts of a chunked host-to-device copy
 };
 
 namespace tsz {
