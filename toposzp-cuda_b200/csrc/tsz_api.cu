@@ -111,11 +111,13 @@ int encode_pass(szp_b200_ctx *ctx, int mode, const float *d_data, const int *d_i
 // over the tiles whose reads (the tile, and one plane -- one row in 2D --
 // beyond it) the copied data already covers.  Tiles leave the launches in
 // order, so the look-back of a launch only meets completed tiles of earlier
-// launches.  Same results as one encode_pass over the whole field.
+// launches.  Same results as one encode_pass over the whole field.  With
+// h_out set, the stream goes to the host part by part on the copy stream as
+// the launches finish (the caller waits for the copy stream).
 static int encode_topo_chunked(szp_b200_ctx *ctx, const float *h_src, float *d_data, unsigned long long n, int B,
                                float eb, const Geom &g, unsigned char *d_stream, unsigned long long stream_cap,
                                unsigned long long *d_blk_off, void *d_cp, unsigned long long cp_cap,
-                               unsigned long long totals_out[3]) {
+                               unsigned long long totals_out[3], unsigned char *h_out, size_t out_cap) {
   cudaStream_t s = ctx->stream;
   cudaStream_t cs = copy_stream(ctx);
   if (!cs) return -1;
@@ -163,6 +165,7 @@ static int encode_topo_chunked(szp_b200_ctx *ctx, const float *h_src, float *d_d
   a.cp_out = d_cp;
   a.cp_cap = cp_cap;
   unsigned long long done = 0;
+  int parts = 0;
   for (int k = 0; k < K; k++) {
     if (cuda_fail(cudaStreamWaitEvent(s, ctx->chunk_ev[k], 0), "wait")) return -1;
     // tiles whose reads end inside [0, cut[k+1])
@@ -176,13 +179,49 @@ static int encode_topo_chunked(szp_b200_ctx *ctx, const float *h_src, float *d_d
     if (cuda_fail(launch_encode(kEncClassify, a, s, grid), "encode launch")) return -1;
     ctx->launches += 1;
     done = upto;
+    if (h_out && upto < ntiles) {
+      // stream bytes through the launch's last tile: its inclusive status word
+      if (!ctx->part_ev[parts] &&
+          cuda_fail(cudaEventCreateWithFlags(&ctx->part_ev[parts], cudaEventDisableTiming), "event"))
+        return -1;
+      if (cuda_fail(cudaMemcpyAsync(ctx->h_words + 32 + parts, &desc[upto - 1].status, 8, cudaMemcpyDeviceToHost,
+                                    s), "D2H") ||
+          cuda_fail(cudaEventRecord(ctx->part_ev[parts], s), "event"))
+        return -1;
+      parts++;
+    }
   }
   if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
-                "D2H totals") ||
-      cuda_fail(cudaStreamSynchronize(s), "encode"))
+                "D2H totals"))
     return -1;
+  // as each launch finishes, its part of the stream leaves for the host on a
+  // stream of its own (the copy stream still carries the field's later parts)
+  cudaStream_t ds = h_out ? d2h_stream(ctx) : nullptr;
+  if (h_out && !ds) return -1;
+  unsigned long long sent = 0;   // stream bytes (header included) already queued
+  for (int p = 0; p < parts; p++) {
+    if (cuda_fail(cudaEventSynchronize(ctx->part_ev[p]), "encode")) return -1;
+    const unsigned long long st = ctx->h_words[32 + p];
+    if ((st >> kStatShift) != 2ull) break;   // not an inclusive prefix: left to the final copy
+    const unsigned long long upto_bytes = 8 + (st & kByteMask);
+    if (upto_bytes > out_cap || upto_bytes > stream_cap) break;
+    if (upto_bytes > sent &&
+        cuda_fail(cudaMemcpyAsync(h_out + sent, d_stream + sent, upto_bytes - sent, cudaMemcpyDeviceToHost, ds),
+                  "D2H stream"))
+      return -1;
+    sent = upto_bytes > sent ? upto_bytes : sent;
+  }
+  if (cuda_fail(cudaStreamSynchronize(s), "encode")) return -1;
   const int err = (int)(ctx->h_words[4] & 0xffffffffu);
   if (err) { set_error("encoder reported status %d", err); return -1; }
+  if (h_out) {
+    const unsigned long long total = 8 + ctx->h_words[0];
+    if (total > out_cap) { set_error("topology output buffer too small (%llu bytes needed)", total); return -1; }
+    if (total > sent &&
+        cuda_fail(cudaMemcpyAsync(h_out + sent, d_stream + sent, total - sent, cudaMemcpyDeviceToHost, ds),
+                  "D2H stream"))
+      return -1;
+  }
   totals_out[0] = ctx->h_words[0];
   totals_out[1] = ctx->h_words[1];
   totals_out[2] = ctx->h_words[2];
@@ -652,7 +691,7 @@ static int compress_dev_impl(szp_b200_ctx *ctx, const float *d_data, szp_b200_ge
     return -1;
   if (chunked ? encode_topo_chunked(ctx, h_src, const_cast<float *>(d_data), n, B, absErrBound, g, d_topo,
                                     stream_bound(n, B, true), reinterpret_cast<unsigned long long *>(d_blk_index),
-                                    pairs, kcap, tot)
+                                    pairs, kcap, tot, h_topo, topo_cap)
               : encode_pass(ctx, kEncClassify, d_data, nullptr, nullptr, n, B, absErrBound, g, d_topo,
                             stream_bound(n, B, true), reinterpret_cast<unsigned long long *>(d_blk_index),
                             kCpPairs, pairs, kcap, tot))
@@ -662,7 +701,7 @@ static int compress_dev_impl(szp_b200_ctx *ctx, const float *d_data, szp_b200_ge
   sizes->cp_count = tot[1];
   sizes->extrema_count = tot[2];
   sizes->sort_bytes = 0;
-  if (h_topo) {
+  if (h_topo && !chunked) {
     // the encoder has finished (encode_pass waited for it): copy now
     if (sizes->topo_bytes > topo_cap) {
       set_error("topology output buffer too small (%zu bytes needed)", sizes->topo_bytes);
@@ -934,19 +973,22 @@ int szp_b200_topo_compress_host(szp_b200_ctx *ctx, const float *h_data, szp_b200
   // stream goes to the host while the rank and sort stages run
   const int rc = compress_dev_impl(ctx, d_data, geom, absErrBound, blockSize, d_topo, d_sort, nullptr, sizes,
                                    h_topo, topo_cap, h_data);
-  cudaStream_t cs = ctx->copy_stream;
+  cudaStream_t cs = ctx->copy_stream, ds = ctx->d2h_stream;
   if (rc) {
     if (cs) cudaStreamSynchronize(cs);
+    if (ds) cudaStreamSynchronize(ds);
     return -1;
   }
   if (sizes->sort_bytes > sort_cap) {
     if (cs) cudaStreamSynchronize(cs);
+    if (ds) cudaStreamSynchronize(ds);
     set_error("sort-position output buffer too small (%zu bytes needed)", sizes->sort_bytes);
     return -1;
   }
   if ((sizes->sort_bytes &&
        cuda_fail(cudaMemcpyAsync(h_sort, d_sort, sizes->sort_bytes, cudaMemcpyDeviceToHost, s), "D2H")) ||
-      cuda_fail(cudaStreamSynchronize(s), "sync") || (cs && cuda_fail(cudaStreamSynchronize(cs), "sync")))
+      cuda_fail(cudaStreamSynchronize(s), "sync") || (cs && cuda_fail(cudaStreamSynchronize(cs), "sync")) ||
+      (ds && cuda_fail(cudaStreamSynchronize(ds), "sync")))
     return -1;
   return 0;
 }

@@ -97,14 +97,25 @@ cudaStream_t copy_stream(szp_b200_ctx *ctx) {
   return ctx->copy_stream;
 }
 
+cudaStream_t d2h_stream(szp_b200_ctx *ctx) {
+  if (!ctx->d2h_stream &&
+      cuda_fail(cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking), "cudaStreamCreate"))
+    return nullptr;
+  return ctx->d2h_stream;
+}
+
 static void ctx_free(szp_b200_ctx *c) {
   if (!c) return;
+  if (c->d2h_stream) { cudaStreamSynchronize(c->d2h_stream); cudaStreamDestroy(c->d2h_stream); }
+  c->d2h_stream = nullptr;
   if (c->copy_stream) { cudaStreamSynchronize(c->copy_stream); cudaStreamDestroy(c->copy_stream); }
   if (c->copy_ev) cudaEventDestroy(c->copy_ev);
   c->copy_stream = nullptr;
   c->copy_ev = nullptr;
   for (int i = 0; i < szp_b200_ctx::kChunkEvents; i++)
     if (c->chunk_ev[i]) { cudaEventDestroy(c->chunk_ev[i]); c->chunk_ev[i] = nullptr; }
+  for (int i = 0; i < szp_b200_ctx::kChunkEvents; i++)
+    if (c->part_ev[i]) { cudaEventDestroy(c->part_ev[i]); c->part_ev[i] = nullptr; }
   for (int i = 0; i <= szp_b200_ctx::kMaxStages; i++)
     if (c->ev[i]) { cudaEventDestroy(c->ev[i]); c->ev[i] = nullptr; }
   c->scratch.release();

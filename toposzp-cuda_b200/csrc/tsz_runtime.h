@@ -54,8 +54,10 @@ struct szp_b200_ctx {
   // second stream for host copies that overlap work on `stream` (created on first use)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t copy_ev = nullptr;
+  cudaStream_t d2h_stream = nullptr;         // device-to-host copies that overlap copy_stream
   static constexpr int kChunkEvents = 16;
   cudaEvent_t chunk_ev[kChunkEvents] = {};   // parts of a chunked host-to-device copy
+  cudaEvent_t part_ev[kChunkEvents] = {};    // encoder launches of a chunked encode
 };
 
 namespace tsz {
@@ -70,6 +72,8 @@ void tl_mark(szp_b200_ctx *ctx, const char *name);
 
 // The workspace's copy stream and its event (created on first use); null on failure.
 cudaStream_t copy_stream(szp_b200_ctx *ctx);
+// A second copy stream for device-to-host copies that run beside copy_stream.
+cudaStream_t d2h_stream(szp_b200_ctx *ctx);
 
 // Rounds a byte count up to 256.
 inline size_t a256(size_t b) { return (b + 255) & ~(size_t)255; }
