@@ -306,3 +306,22 @@ def test_host_compress_in_parts_matches_device(T):
     assert h_topo[: hz.topo_bytes].tobytes() == topo[: sz.topo_bytes].cpu().numpy().tobytes()
     assert h_sort[: hz.sort_bytes].tobytes() == sort[: sz.sort_bytes].cpu().numpy().tobytes()
     ctx.close()
+
+
+@pytest.mark.parametrize("dims", [(128, 128, 128), (224, 224, 224)], ids=["sort_tier", "radix_tier"])
+def test_rank_fallback_tiers(T, ora, dims):
+    """Values up to 1e3 at eb 1e-6 give bins far wider than the shared bitmap
+    of a bucket: at 128^3 every bucket (about 1.7 K points) is ranked by the
+    in-CTA sort, at 224^3 (about 9 K points per bucket) most go to the
+    device-wide radix fallback.  Sort positions must still be bit-exact."""
+    import torch
+    eb = 1e-6
+    d = (synth.small_field(dims, seed=3, kind="noise") * np.float32(1e3)).astype(np.float32)
+    ctx = T.Context()
+    topo, sort, idx, sizes = ctx.compress(torch.from_numpy(d.reshape(-1).copy()).cuda(), dims, eb, 64)
+    ocp = ora.sort_cp(ora.find_cp(d, eb), d)
+    sp = ora.extract_sp(ocp)
+    assert sizes.cp_count == len(ocp)
+    assert sizes.extrema_count == len(sp)
+    assert sort[: sizes.sort_bytes].cpu().numpy().tobytes() == ora.encode_ints(sp, 64)
+    ctx.close()

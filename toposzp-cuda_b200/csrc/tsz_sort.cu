@@ -21,14 +21,21 @@
 
 namespace tsz {
 
-constexpr int kRankThreads = 256;
+constexpr int kRankThreads = 512;
 constexpr int kMaxSlots = 256;
 constexpr int kBitmapWords = 5120;   // 20 KB bitmap + 20 KB prefix per CTA
 
-struct RankRec {
-  uint32_t code;
-  uint32_t dest;
-  int bin;
+// A bucketed record is the critical-point pair itself ({value code, extremum
+// index}).  Its bin is recomputed from the code, or, when the caller supplies
+// bins (batches, whose bins carry per-field offsets, or a given CP list), read
+// from a bin array permuted together with the records.
+struct BinSrc {
+  const int *bins;   // bins in record order, or nullptr
+  float eb;
+  double inv;
+  __device__ __forceinline__ int operator()(const uint2 &r, unsigned long long i) const {
+    return bins ? bins[i] : quant_bin(code_float(r.x), eb, inv);
+  }
 };
 
 // A chunk of records that belongs to one segment (one field of a batch):
@@ -38,43 +45,86 @@ struct SegChunk {
   unsigned long long bbase;
 };
 
-__device__ __forceinline__ int rec_bin(const uint2 &p, const int *bins, unsigned long long k,
-                                       float eb, double inv) {
-  return bins ? bins[k] : quant_bin(code_float(p.x), eb, inv);
+// exclusive scan of one value per thread over a CTA of T threads; the total
+// goes to *total; s_w holds T/32 words and may be reused after the return
+template <int T>
+__device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned *s_w, unsigned *total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) s_w[warp] = inc;
+  __syncthreads();
+  unsigned wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < T / 32; w++) {
+    const unsigned x = s_w[w];
+    if (w < warp) wpre += x;
+    tot += x;
+  }
+  __syncthreads();
+  *total = tot;
+  return wpre + inc - v;
 }
 
 // ---- 1a. per-CTA bucket histogram over a contiguous chunk -----------------
 // (seg != nullptr: CTA c takes chunk seg[c] instead of the c-th uniform chunk)
-__global__ void bucket_hist_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
-                                   unsigned long long K, float eb, double inv, int logNB,
-                                   unsigned long long chunk, unsigned *__restrict__ M,
-                                   const SegChunk *__restrict__ seg = nullptr) {
+constexpr int kHistThreads = 512;
+constexpr int kHistUnroll = 4;
+
+__global__ void __launch_bounds__(kHistThreads)
+bucket_hist_kernel(const uint2 *__restrict__ pairs, BinSrc bin_of, unsigned long long K, int logNB,
+                   unsigned long long chunk, unsigned *__restrict__ M, const SegChunk *__restrict__ seg = nullptr) {
   extern __shared__ unsigned sh[];
   const int NB = 1 << logNB;
   for (int b = threadIdx.x; b < NB; b += blockDim.x) sh[b] = 0;
   __syncthreads();
   const unsigned long long c0 = seg ? seg[blockIdx.x].k0 : blockIdx.x * chunk;
   const unsigned long long c1 = seg ? seg[blockIdx.x].k1 : ((c0 + chunk < K) ? c0 + chunk : K);
-  for (unsigned long long k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
-    const int bin = rec_bin(pairs[k], bins, k, eb, inv);
-    atomicAdd(&sh[(unsigned)bin & (unsigned)(NB - 1)], 1u);
+  for (unsigned long long k = c0 + threadIdx.x; k < c1; k += (unsigned long long)kHistUnroll * kHistThreads) {
+    uint2 r[kHistUnroll];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; u++) {
+      const unsigned long long j = k + (unsigned long long)u * kHistThreads;
+      if (j < c1) r[u] = pairs[j];
+    }
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; u++) {
+      const unsigned long long j = k + (unsigned long long)u * kHistThreads;
+      if (j < c1) atomicAdd(&sh[(unsigned)bin_of(r[u], j) & (unsigned)(NB - 1)], 1u);
+    }
   }
   __syncthreads();
   for (int b = threadIdx.x; b < NB; b += blockDim.x) M[(size_t)blockIdx.x * NB + b] = sh[b];
 }
 
 // ---- 1b. column scan: M[g][b] <- exclusive prefix over g; tot[b] ----------
-__global__ void bucket_colscan_kernel(unsigned *__restrict__ M, int G, int NB,
-                                      unsigned *__restrict__ tot) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= NB) return;
+// rows g0 .. g1-1 of column b, eight loads in flight
+__device__ __forceinline__ unsigned colscan_rows(unsigned *__restrict__ M, unsigned g0, unsigned g1, int NB, int b) {
   unsigned run = 0;
-  for (int g = 0; g < G; g++) {
+  unsigned g = g0;
+  for (; g + 8 <= g1; g += 8) {
+    unsigned v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) v[u] = M[(size_t)(g + u) * NB + b];
+#pragma unroll
+    for (int u = 0; u < 8; u++) { M[(size_t)(g + u) * NB + b] = run; run += v[u]; }
+  }
+  for (; g < g1; g++) {
     const unsigned v = M[(size_t)g * NB + b];
     M[(size_t)g * NB + b] = run;
     run += v;
   }
-  tot[b] = run;
+  return run;
+}
+
+__global__ void bucket_colscan_kernel(unsigned *__restrict__ M, int G, int NB, unsigned *__restrict__ tot) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= NB) return;
+  tot[b] = colscan_rows(M, 0, (unsigned)G, NB, b);
 }
 
 // segmented column scan: bucket b of segment f scans the rows (chunks)
@@ -84,13 +134,7 @@ __global__ void bucket_colscan_seg_kernel(unsigned *__restrict__ M, const unsign
   const long long gb = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gb >= (long long)F * NB) return;
   const int f = (int)(gb / NB), b = (int)(gb % NB);
-  unsigned run = 0;
-  for (unsigned g = crow[f]; g < crow[f + 1]; g++) {
-    const unsigned v = M[(size_t)g * NB + b];
-    M[(size_t)g * NB + b] = run;
-    run += v;
-  }
-  tot[gb] = run;
+  tot[gb] = colscan_rows(M, crow[f], crow[f + 1], NB, b);
 }
 
 // ---- 1c. exclusive scan of bucket totals (one CTA) -------------------------
@@ -119,43 +163,53 @@ __global__ void bucket_start_kernel(const unsigned *__restrict__ tot, int NB,
 // Each CTA walks its chunk in sub-chunks of kSub records: the records are
 // counting-sorted by bucket in shared memory, then written out in that order,
 // so every bucket's records of a sub-chunk form one contiguous run in global
-// memory (consecutive threads store consecutive addresses).
+// memory (consecutive threads store consecutive addresses).  The next
+// sub-chunk's records are loaded while the current one is written out.
 constexpr int kSub = 4096;
 constexpr int kScatterThreads = 512;
+constexpr int kScatterPer = kSub / kScatterThreads;
+
+__host__ __device__ constexpr size_t scatter_smem(int NB) {
+  return (size_t)NB * 16 + (size_t)kSub * 12;
+}
 
 __global__ void __launch_bounds__(kScatterThreads)
-bucket_scatter_sorted_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
-                             unsigned long long K, float eb, double inv, int logNB,
+bucket_scatter_sorted_kernel(const uint2 *__restrict__ pairs, BinSrc bin_of, unsigned long long K, int logNB,
                              unsigned long long chunk, const unsigned *__restrict__ M,
-                             const unsigned long long *__restrict__ start_all, RankRec *__restrict__ recs,
-                             const SegChunk *__restrict__ seg = nullptr) {
-  extern __shared__ unsigned char smx[];
+                             const unsigned long long *__restrict__ start_all, uint2 *__restrict__ recs,
+                             int *__restrict__ rbins, const SegChunk *__restrict__ seg = nullptr) {
+  extern __shared__ unsigned long long smx[];
   const int NB = 1 << logNB;
-  unsigned *run = reinterpret_cast<unsigned *>(smx);          // records of this CTA already written per bucket
-  unsigned *hist = run + NB;                                   // per sub-chunk counts
+  unsigned long long *base = smx;                              // next global position per bucket
+  unsigned *hist = reinterpret_cast<unsigned *>(base + NB);    // per sub-chunk counts
   unsigned *off = hist + NB;                                   // per sub-chunk exclusive offsets
-  RankRec *stage = reinterpret_cast<RankRec *>(off + NB);      // kSub staged records
-  unsigned short *sb = reinterpret_cast<unsigned short *>(stage + kSub);  // bucket of each staged record
-  __shared__ unsigned s_part[kScatterThreads / 32];
-  for (int b = threadIdx.x; b < NB; b += blockDim.x) run[b] = M[(size_t)blockIdx.x * NB + b];
+  uint2 *stage = reinterpret_cast<uint2 *>(off + NB);          // kSub staged records
+  int *sbin = reinterpret_cast<int *>(stage + kSub);           // their bins
+  __shared__ unsigned s_w[kScatterThreads / 32];
   const unsigned long long c0 = seg ? seg[blockIdx.x].k0 : blockIdx.x * chunk;
   const unsigned long long c1 = seg ? seg[blockIdx.x].k1 : ((c0 + chunk < K) ? c0 + chunk : K);
   const unsigned long long *start = start_all + (seg ? seg[blockIdx.x].bbase : 0ull);
+  for (int b = threadIdx.x; b < NB; b += blockDim.x) {
+    base[b] = start[b] + M[(size_t)blockIdx.x * NB + b];
+    hist[b] = 0;
+  }
+  uint2 pr[kScatterPer];
+#pragma unroll
+  for (int u = 0; u < kScatterPer; u++) {
+    const unsigned long long k = c0 + threadIdx.x + u * kScatterThreads;
+    if (k < c1) pr[u] = pairs[k];
+  }
+  __syncthreads();
   for (unsigned long long sub = c0; sub < c1; sub += kSub) {
     const int cnt = (int)((c1 - sub) < (unsigned long long)kSub ? (c1 - sub) : kSub);
-    for (int b = threadIdx.x; b < NB; b += blockDim.x) hist[b] = 0;
-    __syncthreads();
     // bucket and in-bucket slot of each record (slot order within a bucket is irrelevant)
-    uint2 pr[kSub / kScatterThreads];
-    int bn[kSub / kScatterThreads];
-    unsigned slot[kSub / kScatterThreads];
+    int bn[kScatterPer];
+    unsigned slot[kScatterPer];
 #pragma unroll
-    for (int u = 0; u < kSub / kScatterThreads; u++) {
+    for (int u = 0; u < kScatterPer; u++) {
       const int i = threadIdx.x + u * kScatterThreads;
       if (i < cnt) {
-        const unsigned long long k = sub + i;
-        pr[u] = pairs[k];
-        bn[u] = rec_bin(pr[u], bins, k, eb, inv);
+        bn[u] = bin_of(pr[u], sub + i);
         slot[u] = atomicAdd(&hist[(unsigned)bn[u] & (unsigned)(NB - 1)], 1u);
       }
     }
@@ -164,113 +218,88 @@ bucket_scatter_sorted_kernel(const uint2 *__restrict__ pairs, const int *__restr
     {
       const int per = (NB + kScatterThreads - 1) / kScatterThreads;
       const int b0 = threadIdx.x * per;
-      unsigned sum = 0;
+      unsigned sum = 0, total;
       for (int i = 0; i < per; i++) if (b0 + i < NB) sum += hist[b0 + i];
-      unsigned inc = sum;
-      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += v;
-      }
-      if (lane == 31) s_part[warp] = inc;
-      __syncthreads();
-      unsigned wpre = 0;
-      for (int w = 0; w < warp; w++) wpre += s_part[w];
-      unsigned r = wpre + inc - sum;
+      unsigned r = block_excl_scan<kScatterThreads>(sum, s_w, &total);
       for (int i = 0; i < per; i++)
         if (b0 + i < NB) { off[b0 + i] = r; r += hist[b0 + i]; }
     }
     __syncthreads();
 #pragma unroll
-    for (int u = 0; u < kSub / kScatterThreads; u++) {
+    for (int u = 0; u < kScatterPer; u++) {
       const int i = threadIdx.x + u * kScatterThreads;
       if (i < cnt) {
-        const unsigned b = (unsigned)bn[u] & (unsigned)(NB - 1);
-        const unsigned pos = off[b] + slot[u];
-        RankRec r;
-        r.code = pr[u].x;
-        r.dest = pr[u].y;
-        r.bin = bn[u];
-        stage[pos] = r;
-        sb[pos] = (unsigned short)b;
+        const unsigned pos = off[(unsigned)bn[u] & (unsigned)(NB - 1)] + slot[u];
+        stage[pos] = pr[u];
+        sbin[pos] = bn[u];
       }
     }
     __syncthreads();
-    // write in staged (bucket) order: global = start[b] + run[b] + (pos - off[b])
+    // next sub-chunk in flight during the write-out
+    if (sub + kSub < c1) {
+#pragma unroll
+      for (int u = 0; u < kScatterPer; u++) {
+        const unsigned long long k = sub + kSub + threadIdx.x + u * kScatterThreads;
+        if (k < c1) pr[u] = pairs[k];
+      }
+    }
+    // write in staged (bucket) order: global = base[b] + (i - off[b])
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      const unsigned b = sb[i];
-      recs[start[b] + run[b] + (unsigned)(i - off[b])] = stage[i];
+      const int bv = sbin[i];
+      const unsigned b = (unsigned)bv & (unsigned)(NB - 1);
+      const unsigned long long g = base[b] + (unsigned)(i - off[b]);
+      recs[g] = stage[i];
+      if (rbins) rbins[g] = bv;
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < NB; b += blockDim.x) run[b] += hist[b];
+    for (int b = threadIdx.x; b < NB; b += blockDim.x) {
+      base[b] += hist[b];
+      hist[b] = 0;
+    }
     __syncthreads();
-  }
-}
-
-// ---- 1d'. scatter into buckets (unsorted, kept for reference sizes) -------
-__global__ void bucket_scatter_kernel(const uint2 *__restrict__ pairs, const int *__restrict__ bins,
-                                      unsigned long long K, float eb, double inv, int logNB,
-                                      unsigned long long chunk, const unsigned *__restrict__ M,
-                                      const unsigned long long *__restrict__ start,
-                                      RankRec *__restrict__ recs) {
-  extern __shared__ unsigned sh[];
-  const int NB = 1 << logNB;
-  for (int b = threadIdx.x; b < NB; b += blockDim.x) sh[b] = M[(size_t)blockIdx.x * NB + b];
-  __syncthreads();
-  const unsigned long long c0 = blockIdx.x * chunk;
-  const unsigned long long c1 = (c0 + chunk < K) ? c0 + chunk : K;
-  for (unsigned long long k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
-    const uint2 p = pairs[k];
-    const int bin = rec_bin(p, bins, k, eb, inv);
-    const unsigned b = (unsigned)bin & (unsigned)(NB - 1);
-    const unsigned local = atomicAdd(&sh[b], 1u);
-    RankRec r;
-    r.code = p.x;
-    r.dest = p.y;
-    r.bin = bin;
-    recs[start[b] + local] = r;
   }
 }
 
 // ---- 2. per-bucket bitmap rank ---------------------------------------------
-__device__ __forceinline__ unsigned long long block_sum_u64(unsigned long long v, unsigned long long *red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  unsigned long long t = 0;
-  for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += red[i];
-  return t;
-}
+// Records are read in three passes (bin bounds, bitmap, ranks), kRankUnroll
+// loads in flight per thread.
+constexpr int kRankUnroll = 4;
 
 __global__ void __launch_bounds__(kRankThreads)
-bucket_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *__restrict__ start,
+bucket_rank_kernel(const uint2 *__restrict__ recs, BinSrc bin_of, const unsigned long long *__restrict__ start,
                    int logNB, int *__restrict__ out, unsigned *__restrict__ fb_list,
                    unsigned *__restrict__ fb_count) {
   __shared__ unsigned s_min[kMaxSlots], s_max[kMaxSlots], s_wbase[kMaxSlots + 1];
   __shared__ unsigned bm[kBitmapWords];
   __shared__ unsigned pref[kBitmapWords];
+  __shared__ unsigned s_w[kRankThreads / 32];
   __shared__ int s_bmin, s_bmax;
-  __shared__ unsigned s_total_words;
-  __shared__ int s_fail;
   const unsigned b = blockIdx.x;
   const unsigned long long r0 = start[b], r1 = start[b + 1];
   if (r1 == r0) return;
   const unsigned long long cnt = r1 - r0;
+  constexpr unsigned long long kStep = (unsigned long long)kRankUnroll * kRankThreads;
   // bins of this bucket are b + k * NB; slot = k mod kMaxSlots is one-to-one
   // whenever the bucket's bins span fewer than kMaxSlots values of k
   for (int sl = threadIdx.x; sl < kMaxSlots; sl += blockDim.x) { s_min[sl] = 0xffffffffu; s_max[sl] = 0u; }
-  if (threadIdx.x == 0) { s_bmin = 0x7fffffff; s_bmax = (int)0x80000000; s_fail = 0; }
+  if (threadIdx.x == 0) { s_bmin = 0x7fffffff; s_bmax = (int)0x80000000; }
   __syncthreads();
   int lmin = 0x7fffffff, lmax = (int)0x80000000;
-  for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const RankRec r = recs[r0 + i];
-    lmin = min(lmin, r.bin);
-    lmax = max(lmax, r.bin);
-    const int sl = (r.bin >> logNB) & (kMaxSlots - 1);
-    atomicMin(&s_min[sl], r.code);
-    atomicMax(&s_max[sl], r.code);
+  for (unsigned long long i = threadIdx.x; i < cnt; i += kStep) {
+    uint2 r[kRankUnroll];
+#pragma unroll
+    for (int u = 0; u < kRankUnroll; u++)
+      if (i + u * kRankThreads < cnt) r[u] = recs[r0 + i + u * kRankThreads];
+#pragma unroll
+    for (int u = 0; u < kRankUnroll; u++) {
+      if (i + u * kRankThreads >= cnt) continue;
+      const int bn = bin_of(r[u], r0 + i + u * kRankThreads);
+      lmin = min(lmin, bn);
+      lmax = max(lmax, bn);
+      const int sl = (bn >> logNB) & (kMaxSlots - 1);
+      atomicMin(&s_min[sl], r[u].x);
+      atomicMax(&s_max[sl], r[u].x);
+    }
   }
   atomicMin(&s_bmin, lmin);
   atomicMax(&s_bmax, lmax);
@@ -280,59 +309,65 @@ bucket_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *_
     if (threadIdx.x == 0) fb_list[atomicAdd(fb_count, 1u)] = b;
     return;
   }
-  if (threadIdx.x == 0) {
-    unsigned long long w = 0;
-    for (int sl = 0; sl < kMaxSlots; sl++) {
-      s_wbase[sl] = (unsigned)w;
-      if (s_max[sl] >= s_min[sl]) w += ((s_max[sl] - s_min[sl]) >> 5) + 1;
-      if (w > kBitmapWords) { s_fail = 1; break; }
+  // bitmap words of every slot, laid out by an exclusive scan over the slots
+  {
+    unsigned wv = 0;
+    if (threadIdx.x < kMaxSlots && s_max[threadIdx.x] >= s_min[threadIdx.x])
+      wv = ((s_max[threadIdx.x] - s_min[threadIdx.x]) >> 5) + 1;
+    // a slot wider than the bitmap saturates so that the sum cannot wrap
+    if (wv > kBitmapWords + 1) wv = kBitmapWords + 1;
+    unsigned total;
+    const unsigned wb = block_excl_scan<kRankThreads>(wv, s_w, &total);
+    if (total > kBitmapWords) {
+      if (threadIdx.x == 0) fb_list[atomicAdd(fb_count, 1u)] = b;
+      return;
     }
-    s_wbase[kMaxSlots] = (unsigned)w;
-    s_total_words = (unsigned)w;
+    if (threadIdx.x < kMaxSlots) s_wbase[threadIdx.x] = wb;
+    if (threadIdx.x == 0) s_wbase[kMaxSlots] = total;
   }
   __syncthreads();
-  if (s_fail) {
-    if (threadIdx.x == 0) fb_list[atomicAdd(fb_count, 1u)] = b;
-    return;
-  }
-  const unsigned W = s_total_words;
+  const unsigned W = s_wbase[kMaxSlots];
   for (unsigned w = threadIdx.x; w < W; w += blockDim.x) bm[w] = 0u;
   __syncthreads();
-  for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const RankRec r = recs[r0 + i];
-    const int sl = (r.bin >> logNB) & (kMaxSlots - 1);
-    const unsigned pos = r.code - s_min[sl];
-    atomicOr(&bm[s_wbase[sl] + (pos >> 5)], 1u << (pos & 31));
+  for (unsigned long long i = threadIdx.x; i < cnt; i += kStep) {
+    uint2 r[kRankUnroll];
+#pragma unroll
+    for (int u = 0; u < kRankUnroll; u++)
+      if (i + u * kRankThreads < cnt) r[u] = recs[r0 + i + u * kRankThreads];
+#pragma unroll
+    for (int u = 0; u < kRankUnroll; u++) {
+      if (i + u * kRankThreads >= cnt) continue;
+      const int sl = (bin_of(r[u], r0 + i + u * kRankThreads) >> logNB) & (kMaxSlots - 1);
+      const unsigned pos = r[u].x - s_min[sl];
+      atomicOr(&bm[s_wbase[sl] + (pos >> 5)], 1u << (pos & 31));
+    }
   }
   __syncthreads();
   // exclusive prefix popcount over the bitmap words (each thread owns a run)
   {
     const unsigned per = (W + blockDim.x - 1) / blockDim.x;
     const unsigned w0 = threadIdx.x * per;
-    unsigned sm = 0;
+    unsigned sm = 0, total;
     for (unsigned i = 0; i < per; i++) if (w0 + i < W) sm += __popc(bm[w0 + i]);
-    __shared__ unsigned part[kRankThreads];
-    part[threadIdx.x] = sm;
-    __syncthreads();
-    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-      unsigned v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0u;
-      __syncthreads();
-      part[threadIdx.x] += v;
-      __syncthreads();
-    }
-    unsigned run = part[threadIdx.x] - sm;
+    unsigned run = block_excl_scan<kRankThreads>(sm, s_w, &total);
     for (unsigned i = 0; i < per; i++)
       if (w0 + i < W) { pref[w0 + i] = run; run += __popc(bm[w0 + i]); }
   }
   __syncthreads();
-  for (unsigned long long i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const RankRec r = recs[r0 + i];
-    if (r.dest == kNoExtremum) continue;
-    const int sl = (r.bin >> logNB) & (kMaxSlots - 1);
-    const unsigned pos = r.code - s_min[sl];
-    const unsigned w = s_wbase[sl] + (pos >> 5);
-    const unsigned below = __popc(bm[w] & ((1u << (pos & 31)) - 1u));
-    out[r.dest] = (int)(pref[w] - pref[s_wbase[sl]] + below);
+  for (unsigned long long i = threadIdx.x; i < cnt; i += kStep) {
+    uint2 r[kRankUnroll];
+#pragma unroll
+    for (int u = 0; u < kRankUnroll; u++)
+      if (i + u * kRankThreads < cnt) r[u] = recs[r0 + i + u * kRankThreads];
+#pragma unroll
+    for (int u = 0; u < kRankUnroll; u++) {
+      if (i + u * kRankThreads >= cnt || r[u].y == kNoExtremum) continue;
+      const int sl = (bin_of(r[u], r0 + i + u * kRankThreads) >> logNB) & (kMaxSlots - 1);
+      const unsigned pos = r[u].x - s_min[sl];
+      const unsigned w = s_wbase[sl] + (pos >> 5);
+      const unsigned below = __popc(bm[w] & ((1u << (pos & 31)) - 1u));
+      out[r[u].y] = (int)(pref[w] - pref[s_wbase[sl]] + below);
+    }
   }
 }
 
@@ -344,7 +379,7 @@ constexpr int kSortCap = 8192;
 constexpr int kSortThreads = 256;
 
 __global__ void __launch_bounds__(kSortThreads)
-bucket_sort_rank_kernel(const RankRec *__restrict__ recs, const unsigned long long *__restrict__ start,
+bucket_sort_rank_kernel(const uint2 *__restrict__ recs, BinSrc bin_of, const unsigned long long *__restrict__ start,
                         const unsigned *__restrict__ fb_list, const unsigned *__restrict__ fb_count,
                         int *__restrict__ out, unsigned *__restrict__ fb2_list, unsigned *__restrict__ fb2_count) {
   extern __shared__ unsigned long long sk[];
@@ -363,9 +398,9 @@ bucket_sort_rank_kernel(const RankRec *__restrict__ recs, const unsigned long lo
   while (P < cnt) P <<= 1;
   for (unsigned i = threadIdx.x; i < P; i += blockDim.x) {
     if (i < cnt) {
-      const RankRec r = recs[r0 + i];
-      sk[i] = ((unsigned long long)((unsigned)r.bin ^ 0x80000000u) << 32) | r.code;
-      sd[i] = r.dest;
+      const uint2 r = recs[r0 + i];
+      sk[i] = ((unsigned long long)((unsigned)bin_of(r, r0 + i) ^ 0x80000000u) << 32) | r.x;
+      sd[i] = r.y;
     } else {
       sk[i] = ~0ull;
       sd[i] = kNoExtremum;
@@ -433,16 +468,16 @@ __global__ void fb_gather_count_kernel(const unsigned *__restrict__ fb_list, uns
 __global__ void fb_gather_kernel(const unsigned *__restrict__ fb_list, unsigned nfb,
                                  const unsigned long long *__restrict__ start,
                                  const unsigned long long *__restrict__ fb_off,
-                                 const RankRec *__restrict__ recs,
+                                 const uint2 *__restrict__ recs, BinSrc bin_of,
                                  unsigned long long *__restrict__ key,
                                  unsigned *__restrict__ val) {
   for (unsigned f = blockIdx.x; f < nfb; f += gridDim.x) {
     const unsigned long long r0 = start[fb_list[f]], r1 = start[fb_list[f] + 1];
     const unsigned long long o = fb_off[f];
     for (unsigned long long i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      const RankRec r = recs[i];
-      key[o + (i - r0)] = ((unsigned long long)((unsigned)r.bin ^ 0x80000000u) << 32) | r.code;
-      val[o + (i - r0)] = r.dest;
+      const uint2 r = recs[i];
+      key[o + (i - r0)] = ((unsigned long long)((unsigned)bin_of(r, i) ^ 0x80000000u) << 32) | r.x;
+      val[o + (i - r0)] = r.y;
     }
   }
 }
@@ -569,14 +604,52 @@ __global__ void fb_rank_kernel(const unsigned long long *__restrict__ key,
   }
 }
 
-static int rank_fallback(szp_b200_ctx *ctx, RankRec *recs, const unsigned long long *start,
+static int rank_fallback(szp_b200_ctx *ctx, const uint2 *recs, BinSrc bin_of, const unsigned long long *start,
                          const unsigned *fb_list, unsigned nfb, int *d_sp);
+
+// bucket stages shared by the single-field and segmented drivers, launched
+// after the histogram matrix M and the bucket starts exist
+static int rank_buckets(szp_b200_ctx *ctx, const uint2 *d_pairs, BinSrc src, unsigned long long K, int logNB,
+                        unsigned nbk, unsigned C, unsigned long long chunk, const unsigned *M,
+                        const unsigned long long *start, const SegChunk *d_chunks, int *d_sp) {
+  cudaStream_t s = ctx->stream;
+  Arena &A = ctx->scratch;
+  uint2 *recs = A.take<uint2>(K);
+  int *rbins = src.bins ? A.take<int>(K) : nullptr;
+  unsigned *fb_list = A.take<unsigned>(nbk);
+  unsigned *fb2_list = A.take<unsigned>(nbk);
+  unsigned *fb_cnt = A.take<unsigned>(4);
+  if (!recs || (src.bins && !rbins) || !fb_list || !fb2_list || !fb_cnt) {
+    set_error("scratch arena too small for the rank stage");
+    return -1;
+  }
+  const size_t ssm = scatter_smem(1 << logNB);
+  cudaFuncSetAttribute(bucket_scatter_sorted_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm);
+  bucket_scatter_sorted_kernel<<<C, kScatterThreads, ssm, s>>>(d_pairs, src, K, logNB, chunk, M, start, recs,
+                                                               rbins, d_chunks);
+  // past the scatter, bins (when given) are read in record order
+  const BinSrc rsrc = {rbins, src.eb, src.inv};
+  if (cuda_fail(cudaMemsetAsync(fb_cnt, 0, 16, s), "memset")) return -1;
+  bucket_rank_kernel<<<nbk, kRankThreads, 0, s>>>(recs, rsrc, start, logNB, d_sp, fb_list, fb_cnt);
+  cudaFuncSetAttribute(bucket_sort_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_rank_smem());
+  bucket_sort_rank_kernel<<<nbk, kSortThreads, sort_rank_smem(), s>>>(recs, rsrc, start, fb_list, fb_cnt, d_sp,
+                                                                      fb2_list, fb_cnt + 1);
+  ctx->launches += 3;
+  if (cuda_fail(cudaGetLastError(), "rank kernels")) return -1;
+  unsigned nfb = 0;
+  if (cuda_fail(cudaMemcpyAsync(&nfb, fb_cnt + 1, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+      cuda_fail(cudaStreamSynchronize(s), "rank"))
+    return -1;
+  if (nfb == 0) return 0;
+  return rank_fallback(ctx, recs, rsrc, start, fb2_list, nfb, d_sp);
+}
 
 int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
                    unsigned long long K, unsigned long long E, float eb, int *d_sp) {
   if (K == 0) return 0;
+  (void)E;
   cudaStream_t s = ctx->stream;
-  const double inv = 1.0 / (double)eb;
+  const BinSrc src = {d_bins, eb, 1.0 / (double)eb};
   // 2^9 buckets keep each bucket's bins (slots) within the shared bitmap for
   // typical fields while giving the coalesced scatter long runs
   int logNB = 6;
@@ -589,46 +662,21 @@ int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
   unsigned *M = A.take<unsigned>((size_t)G * NB);
   unsigned *tot = A.take<unsigned>(NB);
   unsigned long long *start = A.take<unsigned long long>(NB + 1);
-  RankRec *recs = A.take<RankRec>(K);
-  unsigned *fb_list = A.take<unsigned>(NB);
-  unsigned *fb_cnt = A.take<unsigned>(4);
-  if (!M || !tot || !start || !recs || !fb_list || !fb_cnt) {
+  if (!M || !tot || !start) {
     set_error("scratch arena too small for the rank stage");
     return -1;
   }
   const size_t hsm = (size_t)NB * 4;
-  cudaFuncSetAttribute(bucket_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm);
-  cudaFuncSetAttribute(bucket_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm);
-  bucket_hist_kernel<<<G, 512, hsm, s>>>(d_pairs, d_bins, K, eb, inv, logNB, chunk, M);
+  bucket_hist_kernel<<<G, kHistThreads, hsm, s>>>(d_pairs, src, K, logNB, chunk, M);
   bucket_colscan_kernel<<<(NB + 255) / 256, 256, 0, s>>>(M, G, NB, tot);
   bucket_start_kernel<<<1, 1024, 0, s>>>(tot, NB, start);
-  {
-    const size_t ssm = (size_t)3 * NB * 4 + (size_t)kSub * sizeof(RankRec) + (size_t)kSub * 2 + 64;
-    cudaFuncSetAttribute(bucket_scatter_sorted_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm);
-    bucket_scatter_sorted_kernel<<<G, kScatterThreads, ssm, s>>>(d_pairs, d_bins, K, eb, inv, logNB, chunk, M,
-                                                                 start, recs);
-  }
-  if (cuda_fail(cudaMemsetAsync(fb_cnt, 0, 16, s), "memset")) return -1;
-  bucket_rank_kernel<<<NB, kRankThreads, 0, s>>>(recs, start, logNB, d_sp, fb_list, fb_cnt);
-  unsigned *fb2_list = A.take<unsigned>(NB);
-  if (!fb2_list) { set_error("scratch arena too small for the rank stage"); return -1; }
-  cudaFuncSetAttribute(bucket_sort_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_rank_smem());
-  bucket_sort_rank_kernel<<<NB, kSortThreads, sort_rank_smem(), s>>>(recs, start, fb_list, fb_cnt, d_sp, fb2_list,
-                                                                     fb_cnt + 1);
-  ctx->launches += 6;
-  if (cuda_fail(cudaGetLastError(), "rank kernels")) return -1;
-  unsigned nfb = 0;
-  if (cuda_fail(cudaMemcpyAsync(&nfb, fb_cnt + 1, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
-      cuda_fail(cudaStreamSynchronize(s), "rank"))
-    return -1;
-  if (nfb == 0) return 0;
-  (void)E;
-  return rank_fallback(ctx, recs, start, fb2_list, nfb, d_sp);
+  ctx->launches += 3;
+  return rank_buckets(ctx, d_pairs, src, K, logNB, (unsigned)NB, (unsigned)G, chunk, M, start, nullptr, d_sp);
 }
 
 // Buckets that did not fit the bitmap rank: their records are gathered and
 // ranked after a device-wide LSD radix sort on (bin, code).
-static int rank_fallback(szp_b200_ctx *ctx, RankRec *recs, const unsigned long long *start,
+static int rank_fallback(szp_b200_ctx *ctx, const uint2 *recs, BinSrc bin_of, const unsigned long long *start,
                          const unsigned *fb_list, unsigned nfb, int *d_sp) {
   cudaStream_t s = ctx->stream;
   Arena &A = ctx->scratch;
@@ -652,7 +700,7 @@ static int rank_fallback(szp_b200_ctx *ctx, RankRec *recs, const unsigned long l
     return -1;
   }
   cudaMemcpyAsync(fb_off, h_off.data(), nfb * 8, cudaMemcpyHostToDevice, s);
-  fb_gather_kernel<<<std::min(nfb, 4096u), 256, 0, s>>>(fb_list, nfb, start, fb_off, recs, k1, v1);
+  fb_gather_kernel<<<std::min(nfb, 4096u), 256, 0, s>>>(fb_list, nfb, start, fb_off, recs, bin_of, k1, v1);
   for (int shift = 0; shift < 64; shift += 8) {
     radix_hist_kernel<<<ntiles, 256, 0, s>>>(k1, nf, shift, H, ntiles);
     scan_inplace_kernel<<<1, 1024, 0, s>>>(H, (unsigned long long)256 * ntiles);
@@ -699,10 +747,7 @@ int rank_positions_seg(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bin
   unsigned *M = A.take<unsigned>((size_t)C * NB);
   unsigned *tot = A.take<unsigned>(nbk);
   unsigned long long *start = A.take<unsigned long long>(nbk + 1);
-  RankRec *recs = A.take<RankRec>(K);
-  unsigned *fb_list = A.take<unsigned>(nbk);
-  unsigned *fb_cnt = A.take<unsigned>(4);
-  if (!d_chunks || !d_crow || !M || !tot || !start || !recs || !fb_list || !fb_cnt) {
+  if (!d_chunks || !d_crow || !M || !tot || !start) {
     set_error("scratch arena too small for the batched rank stage");
     return -1;
   }
@@ -711,32 +756,13 @@ int rank_positions_seg(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bin
       cuda_fail(cudaMemcpyAsync(d_crow, crow.data(), (F + 1) * sizeof(unsigned), cudaMemcpyHostToDevice, s),
                 "H2D chunk rows"))
     return -1;
+  const BinSrc src = {d_bins, 1.0f, 1.0};
   const size_t hsm = (size_t)NB * 4;
-  cudaFuncSetAttribute(bucket_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm);
-  bucket_hist_kernel<<<C, 512, hsm, s>>>(d_pairs, d_bins, K, 1.0f, 1.0, logNB, chunk, M, d_chunks);
+  bucket_hist_kernel<<<C, kHistThreads, hsm, s>>>(d_pairs, src, K, logNB, chunk, M, d_chunks);
   bucket_colscan_seg_kernel<<<(unsigned)((nbk + 255) / 256), 256, 0, s>>>(M, d_crow, F, NB, tot);
   bucket_start_kernel<<<1, 1024, 0, s>>>(tot, (int)nbk, start);
-  {
-    const size_t ssm = (size_t)3 * NB * 4 + (size_t)kSub * sizeof(RankRec) + (size_t)kSub * 2 + 64;
-    cudaFuncSetAttribute(bucket_scatter_sorted_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm);
-    bucket_scatter_sorted_kernel<<<C, kScatterThreads, ssm, s>>>(d_pairs, d_bins, K, 1.0f, 1.0, logNB, chunk, M,
-                                                                 start, recs, d_chunks);
-  }
-  if (cuda_fail(cudaMemsetAsync(fb_cnt, 0, 16, s), "memset")) return -1;
-  bucket_rank_kernel<<<(unsigned)nbk, kRankThreads, 0, s>>>(recs, start, logNB, d_sp, fb_list, fb_cnt);
-  unsigned *fb2_list = A.take<unsigned>(nbk);
-  if (!fb2_list) { set_error("scratch arena too small for the batched rank stage"); return -1; }
-  cudaFuncSetAttribute(bucket_sort_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_rank_smem());
-  bucket_sort_rank_kernel<<<(unsigned)nbk, kSortThreads, sort_rank_smem(), s>>>(recs, start, fb_list, fb_cnt, d_sp,
-                                                                                fb2_list, fb_cnt + 1);
-  ctx->launches += 6;
-  if (cuda_fail(cudaGetLastError(), "batched rank kernels")) return -1;
-  unsigned nfb = 0;
-  if (cuda_fail(cudaMemcpyAsync(&nfb, fb_cnt + 1, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
-      cuda_fail(cudaStreamSynchronize(s), "rank"))
-    return -1;
-  if (nfb == 0) return 0;
-  return rank_fallback(ctx, recs, start, fb2_list, nfb, d_sp);
+  ctx->launches += 3;
+  return rank_buckets(ctx, d_pairs, src, K, logNB, (unsigned)nbk, C, chunk, M, start, d_chunks, d_sp);
 }
 
 size_t rank_scratch_bytes_seg(unsigned long long K, int F, int sm_count) {
@@ -746,7 +772,7 @@ size_t rank_scratch_bytes_seg(unsigned long long K, int F, int sm_count) {
   const size_t nbk = (size_t)F * NB;
   const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4);
   return a256(C * sizeof(SegChunk)) + a256((F + 1) * 4) + a256(C * NB * 4) + a256(nbk * 4) +
-         a256((nbk + 1) * 8) + a256(K * sizeof(RankRec)) + a256(nbk * 4) * 2 + a256(16) + fb + a256(nbk * 8) + 8192;
+         a256((nbk + 1) * 8) + a256(K * 8) + a256(K * 4) + a256(nbk * 4) * 2 + a256(16) + fb + a256(nbk * 8) + 8192;
 }
 
 size_t rank_scratch_bytes(unsigned long long K, int sm_count) {
@@ -756,8 +782,9 @@ size_t rank_scratch_bytes(unsigned long long K, int sm_count) {
   const size_t G = (size_t)sm_count * 2 + 1;
   // fallback worst case: all K records (two key/value ping-pong buffers + histogram)
   const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4);
-  return a256(G * NB * 4) + a256(NB * 4) + a256((NB + 1) * 8) + a256(K * sizeof(RankRec)) +
-         a256(NB * 4) * 3 + a256(16) + fb + 4096;
+  // records (8 B) and, for given bins, their permuted bins (4 B)
+  return a256(G * NB * 4) + a256(NB * 4) + a256((NB + 1) * 8) + a256(K * 8) + a256(K * 4) +
+         a256(NB * 4) * 3 + a256(16) + fb + a256((NB + 1) * 8) * 2 + 4096;
 }
 
 // ---------------------------------------------------------------------------
