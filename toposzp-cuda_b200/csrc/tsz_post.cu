@@ -152,19 +152,10 @@ __device__ __forceinline__ float valo(const PostArgs &a, long long e, const C3 &
   return a.F[q];
 }
 
-// every earlier candidate that e may read has its result for this pass
+// every earlier candidate that an RBF / axis-pattern item may read has its
+// result for this pass
 template <int PASS, int ND>
 __device__ bool deps_ready(const PostArgs &a, long long e, const C3 &c) {
-  if (PASS == kPassStencil || PASS == kPassEnforce) {
-    const int nd3 = (ND == 3) ? 1 : 0;
-    const int offs[3][3] = {{-1, 0, 0}, {0, -1, 0}, {0, 0, -1}};
-    for (int k = 1 - nd3; k < 3; k++) {
-      const int dx = offs[k][0], dy = offs[k][1], dz = offs[k][2];
-      const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
-      if (is_cand_known<PASS>(a, q, interior_off(a, c, dx, dy, dz)) && !result_ready(a, q)) return false;
-    }
-    return true;
-  }
   // RBF / axis pattern: earlier points of the 3x3(x3) box and the points two
   // steps back along each axis
   const int xr = (ND == 3) ? 1 : 0;
@@ -195,16 +186,19 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) {
   return v;
 }
 
+// Face neighbours of a stencil / enforcement item as the serial pass sees
+// them: xm, ym, zm (earlier points: results of earlier candidates, else F)
+// and xp, yp, zp (later points: F).  In 2D the x pair is unused.
+struct Face { float xm, xp, ym, yp, zm, zp; };
+
 // 2D stencil (example/test_cuda_topology.cu:118-165)
-__device__ float stencil2(const PostArgs &a, long long e, const C3 &c, int t, int s, float o) {
+__device__ __forceinline__ float stencil2(const PostArgs &a, const Face &f, float cur, int t, int s, float o) {
   const float hi = __fadd_rn(o, a.eb), lo = __fsub_rn(o, a.eb);
-  float m = a.F[e];
-  const int ofs[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+  float m = cur;
+  const float nb[4] = {f.ym, f.yp, f.zm, f.zp};   // rows -1, +1, then columns -1, +1
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const float v = valo<kPassStencil>(a, e, c, 0, ofs[k][0], ofs[k][1]);
-    if (t == 1 ? (v > m) : (v < m)) m = v;
-  }
+  for (int k = 0; k < 4; k++)
+    if (t == 1 ? (nb[k] > m) : (nb[k] < m)) m = nb[k];
   float target;
   if (t == 1) target = __fmul_rn(m, __fadd_rn(1.0f, __fmul_rn((float)s, FLT_EPSILON)));
   else if (s == 0) target = __fmul_rn(m, __fsub_rn(1.0f, FLT_EPSILON));
@@ -213,20 +207,15 @@ __device__ float stencil2(const PostArgs &a, long long e, const C3 &c, int t, in
 }
 
 // 3D stencil (example/test_cuda_topology_3d.cu:77-128)
-__device__ float stencil3(const PostArgs &a, long long e, const C3 &c, int t, int s, float o) {
+__device__ __forceinline__ float stencil3(const PostArgs &a, const Face &f, int t, int s, float o) {
   const float d = __fmul_rn(a.eb, 0.999f);
   const float hi = __fadd_rn(o, d), lo = __fsub_rn(o, d);
-  const long long pl = a.g.plane, d3 = a.g.d3;
-  const float xm = valo<kPassStencil>(a, e, c, -1, 0, 0), xp = a.F[e + pl];
-  const float ym = valo<kPassStencil>(a, e, c, 0, -1, 0), yp = a.F[e + d3];
-  const float zm = valo<kPassStencil>(a, e, c, 0, 0, -1), zp = a.F[e + 1];
-  // later neighbours read through val too (candidates later than e use F)
   float target;
   if (t == 1) {
-    const float m = fmaxf(fmaxf(xm, xp), fmaxf(fmaxf(ym, yp), fmaxf(zm, zp)));
+    const float m = fmaxf(fmaxf(f.xm, f.xp), fmaxf(fmaxf(f.ym, f.yp), fmaxf(f.zm, f.zp)));
     target = __fmul_rn(m, __fadd_rn(1.0f, __fmul_rn((float)s, FLT_EPSILON)));
   } else {
-    const float m = fminf(fminf(xm, xp), fminf(fminf(ym, yp), fminf(zm, zp)));
+    const float m = fminf(fminf(f.xm, f.xp), fminf(fminf(f.ym, f.yp), fminf(f.zm, f.zp)));
     target = (s == 0) ? __fmul_rn(m, __fsub_rn(1.0f, FLT_EPSILON))
                       : __fmul_rn(m, __fsub_rn(1.0f, __fmul_rn(__fdiv_rn(1.0f, (float)s), FLT_EPSILON)));
   }
@@ -235,24 +224,17 @@ __device__ float stencil3(const PostArgs &a, long long e, const C3 &c, int t, in
 
 // enforcement (example/test_cuda_topology.cu:168-198, _3d.cu:131-167)
 template <int ND>
-__device__ float enforce(const PostArgs &a, long long e, const C3 &c, int t, float o) {
+__device__ __forceinline__ float enforce(const PostArgs &a, const Face &f, float cur, int t, float o) {
   const float d = __fmul_rn(a.eb, 0.999f);
   const float hi = __fadd_rn(o, d), lo = __fsub_rn(o, d);
   const float soft = __fmul_rn(0.25f, a.eps);
-  const float cur = a.F[e];
   float m;
   if (ND == 2) {
-    const long long cols = a.g.d3;
-    const float n = valo<kPassEnforce>(a, e, c, 0, -1, 0), s = a.F[e + cols];
-    const float w = valo<kPassEnforce>(a, e, c, 0, 0, -1), ea = a.F[e + 1];
-    m = (t == 1) ? fmaxf(fmaxf(n, s), fmaxf(w, ea)) : fminf(fminf(n, s), fminf(w, ea));
+    // north, south, west, east
+    m = (t == 1) ? fmaxf(fmaxf(f.ym, f.yp), fmaxf(f.zm, f.zp)) : fminf(fminf(f.ym, f.yp), fminf(f.zm, f.zp));
   } else {
-    const long long pl = a.g.plane, d3 = a.g.d3;
-    const float xm = valo<kPassEnforce>(a, e, c, -1, 0, 0), xp = a.F[e + pl];
-    const float ym = valo<kPassEnforce>(a, e, c, 0, -1, 0), yp = a.F[e + d3];
-    const float zm = valo<kPassEnforce>(a, e, c, 0, 0, -1), zp = a.F[e + 1];
-    m = (t == 1) ? fmaxf(fmaxf(xm, xp), fmaxf(fmaxf(ym, yp), fmaxf(zm, zp)))
-                 : fminf(fminf(xm, xp), fminf(fminf(ym, yp), fminf(zm, zp)));
+    m = (t == 1) ? fmaxf(fmaxf(f.xm, f.xp), fmaxf(fmaxf(f.ym, f.yp), fmaxf(f.zm, f.zp)))
+                 : fminf(fminf(f.xm, f.xp), fminf(fminf(f.ym, f.yp), fminf(f.zm, f.zp)));
   }
   if (t == 1) {
     float tg = __fadd_rn(m, soft);
@@ -264,6 +246,45 @@ __device__ float enforce(const PostArgs &a, long long e, const C3 &c, int t, flo
   if (tg < lo) tg = lo;
   if (tg > hi) tg = hi;
   return (cur > tg) ? tg : cur;
+}
+
+// Reads the face neighbours of interior point e for a stencil / enforcement
+// item.  An earlier neighbour that is a candidate of the pass (an interior
+// extremum) must have its result already: its S word carries the value and
+// the pass generation.  Returns false (nothing read is used) while one of them
+// is not final.  Every load is issued before the first wait.
+template <int ND>
+__device__ __forceinline__ bool read_face(const PostArgs &a, long long e, const C3 &c, Face &f) {
+  const long long pl = a.g.plane, d3 = a.g.d3;
+  // earlier neighbours k = 0 (x-1, 3D only), 1 (y-1), 2 (z-1): e is interior,
+  // so each lies in the field and is interior iff its own coordinate is >= 1
+  const long long qb[3] = {e - pl, e - d3, e - 1};
+  const bool inb[3] = {ND == 3 && c.x >= 2, c.y >= 2, c.z >= 2};
+  int tb[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) tb[k] = inb[k] ? (a.T[qb[k]] & 3) : 0;
+  bool cb[3];
+  unsigned long long wb[3];
+  float fb[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    cb[k] = tb[k] == 1 || tb[k] == 2;
+    wb[k] = 0;
+    fb[k] = 0.f;
+    if (ND == 2 && k == 0) continue;
+    if (cb[k]) wb[k] = ld_rlx(&a.S[qb[k]]);
+    else fb[k] = a.F[qb[k]];
+  }
+  f.xp = (ND == 3) ? a.F[e + pl] : 0.f;
+  f.yp = a.F[e + d3];
+  f.zp = a.F[e + 1];
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+    if (cb[k] && (unsigned)(wb[k] >> 32) != a.gen) return false;
+  f.xm = cb[0] ? __uint_as_float((unsigned)wb[0]) : fb[0];
+  f.ym = cb[1] ? __uint_as_float((unsigned)wb[1]) : fb[1];
+  f.zm = cb[2] ? __uint_as_float((unsigned)wb[2]) : fb[2];
+  return true;
 }
 
 __device__ __forceinline__ bool locked(const PostArgs &a, long long q) { return bit_at(a.L, q); }
@@ -735,20 +756,25 @@ template <int PASS, int ND>
 __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx) {
   const long long e = (long long)list[idx];
   const C3 c = coords(a.g, e);
-  if (!deps_ready<PASS, ND>(a, e, c)) return true;
-  const float o = a.OL[idx];
   float r;
   bool ok = false;
-  if (PASS == kPassStencil) {
+  if (PASS == kPassStencil || PASS == kPassEnforce) {
+    const float o = a.OL[idx];
     const int t = ty(a, e);
-    const int s = (idx < a.n_sp) ? a.sp[idx] : 0;
-    r = (ND == 2) ? stencil2(a, e, c, t, s, o) : stencil3(a, e, c, t, s, o);
-  } else if (PASS == kPassEnforce) {
-    r = enforce<ND>(a, e, c, ty(a, e), o);
-  } else if (PASS == kPassRbf) {
-    r = (ND == 2) ? rbf2(a, e, c, o, ok) : rbf3(a, e, c, o, ok);
+    const int s = (PASS == kPassStencil && idx < a.n_sp) ? a.sp[idx] : 0;
+    const float cur = a.F[e];
+    Face f;
+    if (!read_face<ND>(a, e, c, f)) return true;
+    if (PASS == kPassStencil) r = (ND == 2) ? stencil2(a, f, cur, t, s, o) : stencil3(a, f, t, s, o);
+    else r = enforce<ND>(a, f, cur, t, o);
   } else {
-    r = axis3(a, e, c, o, ok);
+    if (!deps_ready<PASS, ND>(a, e, c)) return true;
+    const float o = a.OL[idx];
+    if (PASS == kPassRbf) {
+      r = (ND == 2) ? rbf2(a, e, c, o, ok) : rbf3(a, e, c, o, ok);
+    } else {
+      r = axis3(a, e, c, o, ok);
+    }
   }
   if (ok) atomicAdd(a.restored, 1u);
   // in place: every reader of e's pre-pass value has finished (they are the
@@ -764,7 +790,7 @@ __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__r
 // few times, a block barrier apart, so that chains inside the CTA resolve in
 // this round.  Every thread of the CTA must call it.  Returns true while the
 // item is still pending.
-constexpr int kLocalRetries = 4;
+constexpr int kLocalRetries = 2;
 
 template <int PASS, int ND>
 __device__ __forceinline__ bool pass_item_local(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx,
