@@ -968,23 +968,20 @@ __device__ __forceinline__ unsigned get32(const unsigned *__restrict__ bm, long 
 // within Chebyshev distance 1 (example/test_cuda_topology.cu:229-242,
 // example/test_cuda_topology_3d.cu:325-341): the interior-extremum bitmap E
 // dilated by one along every axis, masked by the interior bitmap I.  The
-// flat-index offsets of the 3x3(x3) neighbourhood become bit offsets, so each
-// output word ORs 9 (2D) or 27 (3D) shifted 32-bit windows of E.  Points that
-// wrap to another row lie on the boundary and are never interior extrema.
-__global__ void lock_bits_kernel(const unsigned *__restrict__ E, const unsigned *__restrict__ I, Geom g,
-                                 long long n, unsigned *__restrict__ L) {
+// 3x3(x3) box is separable, so the dilation runs one axis at a time (flat
+// offsets 1, d3, d2*d3 become bit offsets; each output word ORs three shifted
+// 32-bit windows of the previous stage).  Points that wrap to another row or
+// plane lie on the boundary and are never interior extrema, so no dilated bit
+// crosses a row or plane edge.  I == nullptr: no mask (an intermediate axis).
+__global__ void dilate_bits_kernel(const unsigned *__restrict__ src, long long off, const unsigned *__restrict__ I,
+                                   long long n, unsigned *__restrict__ dst) {
   const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nw = (n + 31) >> 5;
   if (w >= nw) return;
   const long long b0 = w << 5;
-  unsigned acc = 0;
-  const int xr = (g.nd == 3) ? 1 : 0;
-  for (int da = -xr; da <= xr; da++)
-    for (int db = -1; db <= 1; db++) {
-      const long long o = b0 + (long long)da * g.plane + (long long)db * g.d3;
-      acc |= get32(E, o - 1, n) | get32(E, o, n) | get32(E, o + 1, n);
-    }
-  L[w] = acc & I[w];
+  unsigned acc = src[w] | get32(src, b0 - off, n) | get32(src, b0 + off, n);
+  if (I) acc &= I[w];
+  dst[w] = acc;
 }
 
 __global__ void types_from_int_kernel(const int *__restrict__ fn, unsigned char *__restrict__ T, long long n) {
@@ -1186,14 +1183,27 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   tl_mark(ctx, "post_enforce");
   // locks (static: from the types) and the lost saddles (from F after enforcement)
   const long long words = (n + 31) / 32;
-  lock_bits_kernel<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(Eb, Ib, a.g, n, Lb);
+  {
+    // separable dilation of Eb: columns, rows, then planes (3D), with R as
+    // the scratch bitmap (cleared below), masked by Ib at the last axis
+    const unsigned gw = (unsigned)((words + 255) / 256);
+    if (ND == 2) {
+      dilate_bits_kernel<<<gw, 256, 0, s>>>(Eb, 1, nullptr, n, R);
+      dilate_bits_kernel<<<gw, 256, 0, s>>>(R, a.g.d3, Ib, n, Lb);
+    } else {
+      dilate_bits_kernel<<<gw, 256, 0, s>>>(Eb, 1, nullptr, n, Lb);
+      dilate_bits_kernel<<<gw, 256, 0, s>>>(Lb, a.g.d3, nullptr, n, R);
+      dilate_bits_kernel<<<gw, 256, 0, s>>>(R, a.g.plane, Ib, n, Lb);
+    }
+    ctx->launches += ND;
+  }
   if (cuda_fail(cudaMemsetAsync(R, 0, words * 4, s), "memset")) return -1;
   unsigned *ycnt = reinterpret_cast<unsigned *>(ctx->d_words + 8);
   if (cuda_fail(cudaMemsetAsync(ycnt, 0, 4, s), "memset")) return -1;
   a.L = Lb;
   a.R = R;
   if (nz) fn_detect_kernel<<<(nz + 255) / 256, 256, 0, s>>>(a, Z, nz, R, Y, ycnt);
-  ctx->launches += 2;
+  ctx->launches += nz ? 1 : 0;
   if (cuda_fail(cudaGetLastError(), "fn detect")) return -1;
   tl_mark(ctx, "post_fn_locks");
   // RBF runs over Z restricted to the lost saddles (Y holds indices into Z);
