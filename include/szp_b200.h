@@ -169,6 +169,7 @@ SZP_B200_API int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_da
  *                 the block offsets of both streams are then parsed on the
  *                 device from the stream bytes (single-chunk streams, offset
  *                 table [0], as szp_cuda_* and szp_b200_* compressors write)
+ *   d_topo/d_sort any alignment for blockSize <= 256, 4-byte aligned above
  *   d_out         device float[n] (output)
  *   d_types       optional device uint8[n] (2-bit tags, output)
  *   postprocess   0: raw decode only; 1: stencils + enforcement + RBF;

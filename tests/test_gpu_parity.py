@@ -325,3 +325,31 @@ def test_rank_fallback_tiers(T, ora, dims):
     assert sizes.extrema_count == len(sp)
     assert sort[: sizes.sort_bytes].cpu().numpy().tobytes() == ora.encode_ints(sp, 64)
     ctx.close()
+
+
+def test_decompress_unaligned_streams(T):
+    """Device streams may start at any byte for blockSize <= 256 (the decoder
+    stages them through aligned vector loads); blockSize 257 needs 4-byte
+    alignment and reports an error, not a fault, without it."""
+    import torch
+    dims, eb = (40, 50, 60), 1e-3
+    d = torch.from_numpy(field(dims, "bumps", 1.0).reshape(-1).copy()).cuda()
+    ctx = T.Context()
+    topo, sort, idx, sz = ctx.compress(d, dims, eb, 64)
+    ref = ctx.decompress(topo, sz.topo_bytes, sort, sz.sort_bytes, idx, dims, eb, 64).clone()
+    for off in (1, 2, 3, 5, 13):
+        tb = torch.zeros(sz.topo_bytes + 32, dtype=torch.uint8, device="cuda")
+        sb = torch.zeros(sz.sort_bytes + 32, dtype=torch.uint8, device="cuda")
+        tb[off:off + sz.topo_bytes] = topo[:sz.topo_bytes]
+        sb[off:off + sz.sort_bytes] = sort[:sz.sort_bytes]
+        for index in (idx, None):
+            got = ctx.decompress(tb[off:], sz.topo_bytes, sb[off:], sz.sort_bytes, index, dims, eb, 64)
+            assert torch.equal(got.view(torch.int32), ref.view(torch.int32)), (off, index is None)
+    topo3, sort3, idx3, sz3 = ctx.compress(d, dims, eb, 257)
+    tb = torch.zeros(sz3.topo_bytes + 32, dtype=torch.uint8, device="cuda")
+    tb[1:1 + sz3.topo_bytes] = topo3[:sz3.topo_bytes]
+    with pytest.raises(T.ToposzpError):
+        ctx.decompress(tb[1:], sz3.topo_bytes, None, 0, idx3, dims, eb, 257, postprocess=0)
+    ok = ctx.decompress(topo3, sz3.topo_bytes, sort3, sz3.sort_bytes, idx3, dims, eb, 257)
+    assert torch.isfinite(ok).all()
+    ctx.close()

@@ -612,7 +612,7 @@ static cudaError_t launch_dec2(DecArgs a, cudaStream_t s) {
   auto k = decode2_kernel<TAGS, G>;
   const int tb = kWarps * (32 / G);
   const size_t sm = (((size_t)tb * max_block_bytes((uint32_t)a.B, TAGS) + 64) + 15) & ~(size_t)15;
-  a.img_cap = sm - 32;
+  a.img_cap = sm - 48;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const long long nblocks = ((long long)a.n + a.B - 1) / a.B;
@@ -636,6 +636,9 @@ static cudaError_t launch_dec2_tags(DecArgs a, cudaStream_t s) {
 
 cudaError_t launch_decode(bool tags, DecArgs a, cudaStream_t s) {
   if (a.B <= 256) return tags ? launch_dec2_tags<true>(a, s) : launch_dec2_tags<false>(a, s);
+  // the generic decoder stages the payload in 4-byte words: the stream must
+  // start on a 4-byte boundary (the octet decoder takes any alignment)
+  if (reinterpret_cast<uintptr_t>(a.payload) & 3u) return cudaErrorMisalignedAddress;
   a.img_cap = dec_smem_bytes(a.B, tags) - 16;
   return tags ? launch_dec_tags<true>(a, s) : launch_dec_tags<false>(a, s);
 }

@@ -570,32 +570,39 @@ decode2_kernel(DecArgs a) {
     s_off[t] = o;
   }
   __syncthreads();
-  const unsigned long long lo = s_off[0] & ~3ull;
+  // the image holds the payload bytes from the 16-byte boundary at or below
+  // payload + lo: img[ib + k] is payload[lo + k]
+  const unsigned long long lo = s_off[0];
   unsigned long long hi = s_off[nb];
   if (hi > a.payload_len) hi = a.payload_len;
-  if (s_off[0] > hi || hi - lo > a.img_cap) {
+  if (lo > hi || hi - lo > a.img_cap) {
     if (threadIdx.x == 0) atomicExch(a.err, kErrMalformed);
     return;
   }
+  const unsigned ib = (unsigned)(reinterpret_cast<uintptr_t>(a.payload + lo) & 15u);
   {
-    const unsigned long long span = hi - lo;
-    const unsigned long long full_words = (a.payload_len & ~3ull);
-    const uint32_t nw = (uint32_t)((span + 3) >> 2);
-    const uint32_t *srcw = reinterpret_cast<const uint32_t *>(a.payload + lo);
-    uint32_t *imgw = reinterpret_cast<uint32_t *>(img);
-    for (uint32_t w = threadIdx.x; w < nw; w += kThreads) {
-      const unsigned long long gpos = lo + 4ull * w;
-      uint32_t v;
-      if (gpos + 4 <= full_words) {
-        v = __ldg(srcw + w);
+    // addresses as integers: the aligned start may precede the payload
+    const uintptr_t pb = reinterpret_cast<uintptr_t>(a.payload), pe = pb + a.payload_len;
+    const uintptr_t g16 = pb + lo - ib;   // 16-byte aligned
+    const unsigned nq = (ib + (unsigned)(hi - lo) + 15u) >> 4;
+    uint4 *imgq = reinterpret_cast<uint4 *>(img);
+    // a chunk wholly inside [payload, payload + payload_len) is one vector load;
+    // the first and last chunks may reach outside and go byte by byte
+    for (uint32_t q = threadIdx.x; q < nq; q += kThreads) {
+      const uintptr_t src = g16 + 16u * q;
+      uint4 v;
+      if (src >= pb && src + 16 <= pe) {
+        v = __ldg(reinterpret_cast<const uint4 *>(src));
       } else {
-        v = 0;
-        for (int t = 0; t < 4; t++)
-          if (gpos + t < a.payload_len) v |= (uint32_t)a.payload[gpos + t] << (8 * t);
+        uint32_t w4[4] = {0u, 0u, 0u, 0u};
+        for (int t = 0; t < 16; t++)
+          if (src + t >= pb && src + t < pe)
+            w4[t >> 2] |= (uint32_t)(*reinterpret_cast<const unsigned char *>(src + t)) << (8 * (t & 3));
+        v = make_uint4(w4[0], w4[1], w4[2], w4[3]);
       }
-      imgw[w] = v;
+      imgq[q] = v;
     }
-    if (threadIdx.x < 4) imgw[nw + threadIdx.x] = 0;  // padding for 8-byte window reads
+    if (threadIdx.x == 0) imgq[nq] = make_uint4(0u, 0u, 0u, 0u);  // padding for 8-byte window reads
   }
   __syncthreads();
 
@@ -611,8 +618,8 @@ decode2_kernel(DecArgs a) {
   if (ok) {
     if (s_off[bi] < s_off[0] || s_off[bi] + 4 > hi || s_off[bi + 1] < s_off[bi] || s_off[bi + 1] > s_off[nb])
       ok = false;
-    start = (unsigned)(s_off[bi] - lo);
-    bend = (unsigned)((s_off[bi + 1] < hi ? s_off[bi + 1] : hi) - lo);
+    start = (unsigned)(s_off[bi] - lo) + ib;
+    bend = (unsigned)((s_off[bi + 1] < hi ? s_off[bi + 1] : hi) - lo) + ib;
   }
   unsigned bc = 0;
   int anchor = 0;
@@ -640,12 +647,11 @@ decode2_kernel(DecArgs a) {
       const unsigned rsec = mag + fb * (unsigned)cnt;
       // this octet's remainder fields: rem bytes at byte l*rem, MSB first
       const unsigned long long w = ld_bytes8(img, rsec + (unsigned)l * rem);
-      // bytes in stream order -> big-endian integer of rem bytes
-      unsigned long long be = 0;
-#pragma unroll
-      for (int u = 0; u < 7; u++)
-        if ((unsigned)u < rem) be = (be << 8) | ((w >> (8 * u)) & 0xffull);
-      rbits = be;
+      // bytes in stream order -> big-endian integer of rem bytes: byte-swap
+      // the 8-byte window and keep its top rem bytes
+      const unsigned long long sw =
+          ((unsigned long long)__byte_perm((unsigned)w, 0u, 0x0123) << 32) | __byte_perm((unsigned)(w >> 32), 0u, 0x0123);
+      rbits = sw >> (64u - 8u * rem);
     }
     unsigned long long fw = 0;
     if (fb == 1) fw = ld_bytes8(img, mag + (unsigned)e0);
