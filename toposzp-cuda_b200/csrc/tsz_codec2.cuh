@@ -41,6 +41,34 @@ __device__ __forceinline__ void load_oct(const float *__restrict__ p, long long 
   }
 }
 
+// NaN-propagating max / min (PTX max.NaN / min.NaN): NaN when either is NaN
+__device__ __forceinline__ float fmax_nan(float x, float y) {
+  float r;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ float fmin_nan(float x, float y) {
+  float r;
+  asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(x), "f"(y));
+  return r;
+}
+
+// bit t of an 8-bit mask -> bit 2t
+__device__ __forceinline__ unsigned spread2(unsigned x) {
+  x = (x | (x << 4)) & 0x0F0Fu;
+  x = (x | (x << 2)) & 0x3333u;
+  x = (x | (x << 1)) & 0x5555u;
+  return x;
+}
+// bit 2t -> bit t (the inverse of spread2 on the even bits)
+__device__ __forceinline__ unsigned compact2(unsigned x) {
+  x &= 0x5555u;
+  x = (x | (x >> 1)) & 0x3333u;
+  x = (x | (x >> 2)) & 0x0F0Fu;
+  x = (x | (x >> 4)) & 0x00FFu;
+  return x;
+}
+
 // 2-bit types of an octet (element t in bits 2t..2t+1); c[] holds the values
 // of the octet, nv of them valid, i0 the flat index of element 0
 __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, long long n, long long i0,
@@ -78,67 +106,53 @@ __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, 
   for (int t = 0; t < 8; t++)
     if (t == nv - 1 && (inter & (1u << t))) next = __ldg(d + i0 + nv);
   const long long o1 = (g.nd == 2) ? g.d3 : g.plane;  // first axis: rows (2D) or planes (3D)
-  unsigned all_gt = inter, all_lt = inter, any_hi = 0, any_lo = 0, hi_a = 0, lo_a = 0;
+  // Per axis, hi: c above both neighbours, lo: c below both.  c > max(m, p)
+  // with a NaN-propagating max is exactly (c > m && c > p), NaNs included
+  // (any NaN makes both false), and likewise for lo with min.
+  unsigned hi_a = 0, lo_a = 0, hi_b = 0, lo_b = 0, hi_c = 0, lo_c = 0;
   {
     float m[8], p[8];
     load_oct(d, i0 - o1, n, inter, m);
     load_oct(d, i0 + o1, n, inter, p);
 #pragma unroll
     for (int t = 0; t < 8; t++) {
-      const unsigned b = 1u << t;
-      if (!(inter & b)) continue;
-      const bool gm = c[t] > m[t], gp = c[t] > p[t], lm = c[t] < m[t], lp = c[t] < p[t];
-      if (!(gm && gp)) all_gt &= ~b;
-      if (!(lm && lp)) all_lt &= ~b;
-      if (gm && gp) hi_a |= b;
-      if (lm && lp) lo_a |= b;
+      if (!(inter & (1u << t))) continue;
+      if (c[t] > fmax_nan(m[t], p[t])) hi_a |= 1u << t;
+      if (c[t] < fmin_nan(m[t], p[t])) lo_a |= 1u << t;
     }
   }
-  unsigned hi_b = 0, lo_b = 0;
   if (g.nd == 3) {
     float m[8], p[8];
     load_oct(d, i0 - g.d3, n, inter, m);
     load_oct(d, i0 + g.d3, n, inter, p);
 #pragma unroll
     for (int t = 0; t < 8; t++) {
-      const unsigned b = 1u << t;
-      if (!(inter & b)) continue;
-      const bool gm = c[t] > m[t], gp = c[t] > p[t], lm = c[t] < m[t], lp = c[t] < p[t];
-      if (!(gm && gp)) all_gt &= ~b;
-      if (!(lm && lp)) all_lt &= ~b;
-      if (gm && gp) hi_b |= b;
-      if (lm && lp) lo_b |= b;
+      if (!(inter & (1u << t))) continue;
+      if (c[t] > fmax_nan(m[t], p[t])) hi_b |= 1u << t;
+      if (c[t] < fmin_nan(m[t], p[t])) lo_b |= 1u << t;
     }
   }
-  unsigned hi_c = 0, lo_c = 0;
 #pragma unroll
   for (int t = 0; t < 8; t++) {
-    const unsigned b = 1u << t;
-    if (!(inter & b)) continue;
+    if (!(inter & (1u << t))) continue;
     const float lf = (t == 0) ? prev : c[t - 1 < 0 ? 0 : t - 1];
     const float rt = (t == nv - 1) ? next : c[t + 1 > 7 ? 7 : t + 1];
-    const bool gm = c[t] > lf, gp = c[t] > rt, lm = c[t] < lf, lp = c[t] < rt;
-    if (!(gm && gp)) all_gt &= ~b;
-    if (!(lm && lp)) all_lt &= ~b;
-    if (gm && gp) hi_c |= b;
-    if (lm && lp) lo_c |= b;
+    if (c[t] > fmax_nan(lf, rt)) hi_c |= 1u << t;
+    if (c[t] < fmin_nan(lf, rt)) lo_c |= 1u << t;
   }
-  const unsigned mx = all_gt, mn = all_lt & ~mx;
-  unsigned sd;
+  unsigned mx, mn, sd;
   if (g.nd == 2) {
     // vertical axis (rows) is a, horizontal (columns) is c
+    mx = hi_a & hi_c;
+    mn = lo_a & lo_c & ~mx;
     sd = ((lo_a & hi_c) | (hi_a & lo_c)) & ~mx & ~mn;
   } else {
+    mx = hi_a & hi_b & hi_c;
+    mn = lo_a & lo_b & lo_c & ~mx;
     sd = (hi_a | hi_b | hi_c) & (lo_a | lo_b | lo_c) & ~mx & ~mn;
   }
-  unsigned types = 0;
-#pragma unroll
-  for (int t = 0; t < 8; t++) {
-    const unsigned b = 1u << t;
-    const unsigned ty = (mx & b) ? 1u : (mn & b) ? 2u : (sd & b) ? 3u : 0u;
-    types |= ty << (2 * t);
-  }
-  return types;
+  // 2-bit types from the disjoint masks: maximum 01, minimum 10, saddle 11
+  return spread2(mx | sd) | (spread2(mn | sd) << 1);
 }
 
 // CTA-wide exclusive scan of one value per thread (WARPS warps);
@@ -262,12 +276,10 @@ __device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long t
     if (l == 0) s_bytes[bi] = len ? block_bytes((unsigned)len, bc, tags) : 0u;
     unsigned cpm = 0, exm = 0;
     if (MODE == kEncClassify) {
-#pragma unroll
-      for (int t = 0; t < 8; t++) {
-        const unsigned ty = (types >> (2 * t)) & 3u;
-        if (ty) cpm |= 1u << t;
-        if (ty == 1u || ty == 2u) exm |= 1u << t;
-      }
+      // type 01 / 10: extremum, 11: saddle
+      const unsigned lo2 = types & 0x5555u, hi2 = (types >> 1) & 0x5555u;
+      cpm = compact2(lo2 | hi2);
+      exm = compact2(lo2 ^ hi2);
     }
     __syncthreads();
 
@@ -642,35 +654,32 @@ decode2_kernel(DecArgs a) {
     const unsigned negb = img[p + l];
     const unsigned mag = p + sbytes;
     const unsigned fb = bc >> 3, rem = bc & 7u;
-    unsigned long long rbits = 0;
-    if (rem) {
-      const unsigned rsec = mag + fb * (unsigned)cnt;
-      // this octet's remainder fields: rem bytes at byte l*rem, MSB first
-      const unsigned long long w = ld_bytes8(img, rsec + (unsigned)l * rem);
-      // bytes in stream order -> big-endian integer of rem bytes: byte-swap
-      // the 8-byte window and keep its top rem bytes
-      const unsigned long long sw =
-          ((unsigned long long)__byte_perm((unsigned)w, 0u, 0x0123) << 32) | __byte_perm((unsigned)(w >> 32), 0u, 0x0123);
-      rbits = sw >> (64u - 8u * rem);
-    }
-    unsigned long long fw = 0;
-    if (fb == 1) fw = ld_bytes8(img, mag + (unsigned)e0);
+    // Branch-free for the common widths (fb <= 1), so that the blocks of a
+    // warp, which have their own bit counts, do not serialise: the remainder
+    // window is read even when rem == 0 (its address then is the end of the
+    // magnitude section, inside the image) and masked to nothing.
+    const unsigned rsec = mag + fb * (unsigned)cnt;
+    // this octet's remainder fields: rem bytes at byte l*rem, MSB first;
+    // bytes in stream order -> big-endian integer: byte-swap the 8-byte
+    // window and keep its top rem bytes
+    const unsigned long long w = ld_bytes8(img, rsec + (unsigned)l * rem);
+    const unsigned long long sw =
+        ((unsigned long long)__byte_perm((unsigned)w, 0u, 0x0123) << 32) | __byte_perm((unsigned)(w >> 32), 0u, 0x0123);
+    const unsigned long long rbits = rem ? (sw >> (64u - 8u * rem)) : 0ull;
+    const unsigned long long fw = (fb == 1) ? ld_bytes8(img, mag + (unsigned)e0) : 0ull;
+    const unsigned rmask = (1u << rem) - 1u;
 #pragma unroll
     for (int t = 0; t < 8; t++) {
-      if (e0 + t < cnt) {
-        unsigned v = 0;
-        if (rem) v = (unsigned)(rbits >> (rem * (7u - t))) & ((1u << rem) - 1u);
-        if (fb == 1) {
-          v |= (unsigned)((fw >> (8 * t)) & 0xffull) << rem;
-        } else if (fb) {
-          unsigned full = 0;
-          const unsigned o = mag + (unsigned)(e0 + t) * fb;
-          for (unsigned u = 0; u < fb; u++) full |= (unsigned)img[o + u] << (8 * u);
-          v |= full << rem;
-        }
-        dl[t] = ((negb >> (7 - t)) & 1u) ? (0u - v) : v;
-        tsum += dl[t];
+      unsigned v = ((unsigned)(rbits >> (rem * (7u - t))) & rmask) | (((unsigned)(fw >> (8 * t)) & 0xffu) << rem);
+      if (fb >= 2 && e0 + t < cnt) {
+        unsigned full = 0;
+        const unsigned o = mag + (unsigned)(e0 + t) * fb;
+        for (unsigned u = 0; u < fb; u++) full |= (unsigned)img[o + u] << (8 * u);
+        v |= full << rem;
       }
+      const unsigned neg = (negb >> (7 - t)) & 1u;
+      dl[t] = (e0 + t < cnt) ? ((v ^ (0u - neg)) + neg) : 0u;
+      tsum += dl[t];
     }
   }
   // exclusive scan of the octet sums inside the group
