@@ -550,9 +550,14 @@ size_t enc2_smem_bytes(int B, bool tags, bool classify) {
 }
 
 template <int MODE, int G>
-static cudaError_t launch_enc2(const EncArgs &a, cudaStream_t s, int grid) {
+static cudaError_t launch_enc2(const EncArgs &a0, cudaStream_t s, int grid) {
   auto k = encode2_kernel<MODE, G>;
-  const size_t sm = enc2_smem_bytes(a.B, MODE != kEncInts, MODE == kEncClassify);
+  EncArgs a = a0;
+  const size_t one = enc2_smem_bytes(a.B, MODE != kEncInts, MODE == kEncClassify);
+  // two tile images (pipelined look-back) unless the record CP mode is on
+  const bool two = !(MODE == kEncClassify && a.cp_mode == kCpRecords);
+  a.img_stride = two ? (unsigned)one : 0u;
+  const size_t sm = two ? 2 * one : one;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   k<<<grid, kThreads, sm, s>>>(a);

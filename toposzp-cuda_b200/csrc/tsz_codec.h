@@ -28,6 +28,7 @@ struct EncArgs {
   int cp_mode;                  // CpMode (kEncClassify only)
   void *cp_out;                 // CriticalPoint / CriticalPoint3D records or uint2 pairs
   unsigned long long cp_cap;
+  unsigned img_stride;          // octet encoder: bytes of one of its two tile images (0: one image, no pipelining)
 };
 
 struct DecArgs {

@@ -192,11 +192,21 @@ struct EncShared {
   unsigned tile_bytes, tile_cps, tile_ext;
 };
 
-// Encodes tile `tile` (TB codec blocks) of the field described by `a`: all
-// threads of the CTA call it; it ends with a CTA barrier.
+// Per-thread values of a tile that the record mode of phase 6 reads after
+// the look-back (only the unpipelined path keeps them).
+struct EncRegs {
+  unsigned types, cpm, cpo, exo;
+  long long i0;
+};
+
+// Front half of a tile (phases 1-3): quantize, classify, pack the tile image
+// into img, stage the critical-point pairs behind it and publish the tile's
+// aggregate.  All threads of the CTA call it.  The look-back and write-out
+// (encode2_back) may follow at once or after the next tile's front half, on
+// a different image and EncShared.
 template <int MODE, int G, int WARPS>
-__device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long tile, unsigned char *img,
-                                             EncShared<G, WARPS> &sh) {
+__device__ __forceinline__ void encode2_front(const EncArgs &a, const long long tile, unsigned char *img,
+                                              EncShared<G, WARPS> &sh, EncRegs &rg) {
   constexpr int BPW = 32 / G;
   constexpr int TB = WARPS * BPW;
   uint32_t *s_bytes = sh.bytes;
@@ -387,6 +397,34 @@ __device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long t
       }
     }
 
+    rg.types = types;
+    rg.cpm = cpm;
+    rg.cpo = cpo;
+    rg.exo = exo;
+    rg.i0 = i0;
+  }
+}
+
+// Back half of a tile (phases 4-6): decoupled look-back for the tile's stream
+// and CP offsets, block index, write-out of the image staged by
+// encode2_front, copy-out of the staged pairs.  rg: the front half's
+// per-thread values, required for the record CP mode (nullptr otherwise).
+// All threads of the CTA call it; it ends with a CTA barrier.
+template <int MODE, int G, int WARPS>
+__device__ __forceinline__ void encode2_back(const EncArgs &a, const long long tile, unsigned char *img,
+                                             EncShared<G, WARPS> &sh, const EncRegs *rg) {
+  constexpr int BPW = 32 / G;
+  constexpr int TB = WARPS * BPW;
+  uint32_t *s_bytes = sh.bytes;
+  const bool tags = (MODE != kEncInts);
+  uint32_t *imgw = reinterpret_cast<uint32_t *>(img);
+  const long long n = (long long)a.n;
+  const int B = a.B;
+  const long long nblocks = (n + B - 1) / B;
+  const long long ntiles = (nblocks + TB - 1) / TB;
+  const unsigned tile_bytes = sh.tile_bytes;
+  const uint2 *cp_stage = reinterpret_cast<const uint2 *>(img + enc2_img_bytes(B, tags, TB));
+  {
     // ---- phase 4: look-back (whole CTA) ----
     {
       const Prefix pf = lookback_cta<WARPS>(a.desc, tile, tile_bytes,
@@ -449,9 +487,11 @@ __device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long t
           reinterpret_cast<uint2 *>(a.cp_out)[cb + k] = pr;
         }
       }
-    } else if (MODE == kEncClassify && a.cp_mode == kCpRecords && cpm) {
-      unsigned long long ci = (sh.gcnt >> 32) + cpo;
-      unsigned long long ei = (sh.gcnt & 0xffffffffull) + exo;
+    } else if (MODE == kEncClassify && a.cp_mode == kCpRecords && rg && rg->cpm) {
+      const unsigned types = rg->types, cpm = rg->cpm;
+      const long long i0 = rg->i0;
+      unsigned long long ci = (sh.gcnt >> 32) + rg->cpo;
+      unsigned long long ei = (sh.gcnt & 0xffffffffull) + rg->exo;
 #pragma unroll
       for (int t = 0; t < 8; t++) {
         if (!(cpm & (1u << t))) continue;
@@ -486,29 +526,63 @@ __device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long t
   }
 }
 
+// Encodes tile `tile` (TB codec blocks) of the field described by `a`: all
+// threads of the CTA call it; it ends with a CTA barrier.
+template <int MODE, int G, int WARPS>
+__device__ __forceinline__ void encode2_tile(const EncArgs &a, const long long tile, unsigned char *img,
+                                             EncShared<G, WARPS> &sh) {
+  EncRegs rg;
+  encode2_front<MODE, G, WARPS>(a, tile, img, sh, rg);
+  encode2_back<MODE, G, WARPS>(a, tile, img, sh, &rg);
+}
+
 // One field: persistent CTAs claim tiles from a.tile_ctr in order (within
 // [a.tile_lo, a.tile_hi) when a.tile_hi is set: a launch per part of the
-// field, earlier tiles complete).
+// field).  With a.img_stride set the CTA keeps two tile images and runs one
+// tile behind: it publishes tile k's aggregate (front half) before it looks
+// back for tile k-1 and writes that one out, so the look-back's wait overlaps
+// a tile of work.  A CTA waits only after publishing the aggregates of every
+// tile it holds, and tiles are claimed in order, so every tile a look-back
+// waits for belongs to a running CTA that is not waiting.  The record CP mode
+// (per-thread values needed after the look-back) takes the unpipelined loop.
 template <int MODE, int G>
 __global__ void __launch_bounds__(kThreads, (MODE == kEncClassify ? 3 : 4))
 encode2_kernel(EncArgs a) {
   extern __shared__ __align__(16) unsigned char smem_dyn[];
-  __shared__ EncShared<G, kWarps> sh;
+  __shared__ EncShared<G, kWarps> sh[2];
+  __shared__ long long s_claim;
   const long long nblocks = ((long long)a.n + a.B - 1) / a.B;
   const long long ntiles = (nblocks + EncShared<G, kWarps>::TB - 1) / EncShared<G, kWarps>::TB;
+  const long long tend = a.tile_hi ? (long long)a.tile_hi : ntiles;
+  if (a.img_stride == 0 || (MODE == kEncClassify && a.cp_mode == kCpRecords)) {
+    while (true) {
+      if (threadIdx.x == 0) s_claim = (long long)a.tile_lo + (long long)atomicAdd(a.tile_ctr, 1u);
+      __syncthreads();
+      const long long tile = s_claim;
+      if (tile >= tend) break;
+      encode2_tile<MODE, G, kWarps>(a, tile, smem_dyn, sh[0]);
+    }
+    return;
+  }
+  long long prev = -1;
+  int cur = 0;
   while (true) {
-    if (threadIdx.x == 0) sh.tile = (long long)a.tile_lo + (long long)atomicAdd(a.tile_ctr, 1u);
+    if (threadIdx.x == 0) s_claim = (long long)a.tile_lo + (long long)atomicAdd(a.tile_ctr, 1u);
     __syncthreads();
-    const long long tile = sh.tile;
-    if (tile >= (a.tile_hi ? (long long)a.tile_hi : ntiles)) break;
-    encode2_tile<MODE, G, kWarps>(a, tile, smem_dyn, sh);
+    const long long tile = s_claim;
+    const bool more = tile < tend;
+    if (more) {
+      EncRegs rg;
+      encode2_front<MODE, G, kWarps>(a, tile, smem_dyn + (size_t)cur * a.img_stride, sh[cur], rg);
+    }
+    if (prev >= 0)
+      encode2_back<MODE, G, kWarps>(a, prev, smem_dyn + (size_t)(cur ^ 1) * a.img_stride, sh[cur ^ 1], nullptr);
+    if (!more) break;
+    prev = tile;
+    cur ^= 1;
   }
 }
 
-// Many fields in one persistent launch: a device tile work-queue.  Tile t of
-// the queue is tile t - tile_start[f] of field f (tile_start[f] <= t <
-// tile_start[f+1]); a field's tiles leave the queue in order, so its
-// look-back always waits on tiles already held by running CTAs.
 template <int MODE, int G, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, (MODE == kEncClassify ? 24 : 32) / WARPS)
 encode2_batch_kernel(const EncArgs *__restrict__ fields, const unsigned long long *__restrict__ tile_start,
