@@ -78,6 +78,7 @@ struct PostArgs {
   unsigned long long *S;        // (generation << 32) | result bits, per point
   const unsigned *L;            // lock bitmap: interior point next to an interior extremum
   const unsigned *R;            // RBF candidates (lost saddles) bitmap
+  const unsigned *X;            // interior-extremum bitmap (the stencil / enforcement candidates)
   int *err;
   unsigned *restored;
 };
@@ -250,25 +251,22 @@ __device__ __forceinline__ float enforce(const PostArgs &a, const Face &f, float
 
 // Reads the face neighbours of interior point e for a stencil / enforcement
 // item.  An earlier neighbour that is a candidate of the pass (an interior
-// extremum) must have its result already: its S word carries the value and
-// the pass generation.  Returns false (nothing read is used) while one of them
-// is not final.  Every load is issued before the first wait.
+// extremum: a bit of X) must have its result already: its S word carries the
+// value and the pass generation.  Returns false (nothing read is used) while
+// one of them is not final.  Every load is issued before the first wait.
 template <int ND>
-__device__ __forceinline__ bool read_face(const PostArgs &a, long long e, const C3 &c, Face &f) {
+__device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &f) {
   const long long pl = a.g.plane, d3 = a.g.d3;
   // earlier neighbours k = 0 (x-1, 3D only), 1 (y-1), 2 (z-1): e is interior,
-  // so each lies in the field and is interior iff its own coordinate is >= 1
+  // so each lies in the field
   const long long qb[3] = {e - pl, e - d3, e - 1};
-  const bool inb[3] = {ND == 3 && c.x >= 2, c.y >= 2, c.z >= 2};
-  int tb[3];
-#pragma unroll
-  for (int k = 0; k < 3; k++) tb[k] = inb[k] ? (a.T[qb[k]] & 3) : 0;
   bool cb[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) cb[k] = (ND == 3 || k > 0) && bit_at(a.X, qb[k]);
   unsigned long long wb[3];
   float fb[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    cb[k] = tb[k] == 1 || tb[k] == 2;
     wb[k] = 0;
     fb[k] = 0.f;
     if (ND == 2 && k == 0) continue;
@@ -755,7 +753,6 @@ __global__ void fn_detect_kernel(PostArgs a, const unsigned *__restrict__ Z, uns
 template <int PASS, int ND>
 __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx) {
   const long long e = (long long)list[idx];
-  const C3 c = coords(a.g, e);
   float r;
   bool ok = false;
   if (PASS == kPassStencil || PASS == kPassEnforce) {
@@ -764,10 +761,11 @@ __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__r
     const int s = (PASS == kPassStencil && idx < a.n_sp) ? a.sp[idx] : 0;
     const float cur = a.F[e];
     Face f;
-    if (!read_face<ND>(a, e, c, f)) return true;
+    if (!read_face<ND>(a, e, f)) return true;
     if (PASS == kPassStencil) r = (ND == 2) ? stencil2(a, f, cur, t, s, o) : stencil3(a, f, t, s, o);
     else r = enforce<ND>(a, f, cur, t, o);
   } else {
+    const C3 c = coords(a.g, e);
     if (!deps_ready<PASS, ND>(a, e, c)) return true;
     const float o = a.OL[idx];
     if (PASS == kPassRbf) {
@@ -1169,6 +1167,7 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   cudaStream_t s = ctx->stream;
   const long long n = a.n;
   a.OL = OX;
+  a.X = Eb;
   if (a.sp && a.n_sp > 0) {
     a.gen = next_gen(ctx);
     const int rc = run_pass_coop<kPassStencil, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
