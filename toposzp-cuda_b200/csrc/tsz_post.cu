@@ -27,6 +27,7 @@
 
 #include "tsz_lookback.cuh"
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "tsz_ops.h"
@@ -988,8 +989,11 @@ __global__ void types_from_int_kernel(const int *__restrict__ fn, unsigned char 
 }
 
 static bool g_weights_ready[64];
+static std::mutex g_weights_mu;
 
+// once per device; contexts on several host threads may get here together
 static cudaError_t upload_weights(int dev) {
+  std::lock_guard<std::mutex> lk(g_weights_mu);
   if (dev >= 0 && dev < 64 && g_weights_ready[dev]) return cudaSuccess;
   // Gaussian weights in double with the reference formula
   // (example/test_cuda_topology.cu:259-265, example/test_cuda_topology_3d.cu:360-367)
