@@ -356,8 +356,15 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
           }
           p += sbytes;
           const unsigned fb = bc >> 3, rem = bc & 7u;
-          if (fb) {
-            if (has_d) {
+          // Predicated fixed-count stores rather than loops over fb / rem:
+          // the blocks of a warp have their own bit counts, and loops with
+          // per-block trip counts would run one after the other.
+          if (has_d) {
+            // full magnitude bytes: one byte per delta when fb == 1
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+              if (fb == 1 && e0 + t < cnt) img[p + (unsigned)(e0 + t)] = (unsigned char)(mags[t] >> rem);
+            if (fb >= 2) {
 #pragma unroll
               for (int t = 0; t < 8; t++) {
                 if (e0 + t < cnt) {
@@ -367,8 +374,8 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
                 }
               }
             }
-            p += fb * (unsigned)cnt;
           }
+          p += fb * (unsigned)cnt;
           if (rem) {
             const unsigned rbytes = (rem * (unsigned)cnt - 1u) / 8u + 1u;
             if (has_d) {
@@ -378,8 +385,9 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
               for (int t = 0; t < 8; t++) acc = (acc << rem) | (unsigned long long)(mags[t] & mask);
               // the octet's 8*rem bits are exactly rem bytes at byte l*rem
               const unsigned ob = (unsigned)l * rem;
-              for (unsigned u = 0; u < rem; u++)
-                if (ob + u < rbytes) img[p + ob + u] = (unsigned char)(acc >> (8 * (rem - 1u - u)));
+#pragma unroll
+              for (unsigned u = 0; u < 7; u++)
+                if (u < rem && ob + u < rbytes) img[p + ob + u] = (unsigned char)(acc >> (8 * (rem - 1u - u)));
             }
             p += rbytes;
           }
