@@ -179,13 +179,38 @@ __device__ __forceinline__ unsigned cta_excl_scan(unsigned v, unsigned *s_warp, 
   return wpre + inc - v;
 }
 
+// CTA-wide exclusive scan of one 64-bit value per thread (packed fields that
+// never carry into each other); returns the exclusive prefix, total in *total
+template <int WARPS>
+__device__ __forceinline__ unsigned long long cta_excl_scan64(unsigned long long v, unsigned long long *s_warp,
+                                                              unsigned long long *total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  unsigned long long wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < WARPS; w++) {
+    const unsigned long long sw = s_warp[w];
+    if (w < warp) wpre += sw;
+    tot += sw;
+  }
+  *total = tot;
+  return wpre + inc - v;
+}
+
 // Shared state of one encoder CTA (WARPS warps, codec blocks of at most 8G
 // elements, 32/G blocks per warp).
 template <int G, int WARPS>
 struct EncShared {
   static constexpr int TB = WARPS * (32 / G);
   uint32_t bytes[TB];
-  unsigned w1[WARPS], w2[WARPS], w3[WARPS];
+  unsigned long long w64[WARPS];
   long long tile;
   int field;
   unsigned long long gbyte, gcnt;
@@ -294,11 +319,24 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
     __syncthreads();
 
     // ---- phase 2: tile scans (block bytes; per-thread CP / extremum counts) ----
+    // one scan of the three counts packed into 64 bits: block bytes in bits
+    // 0..23 (a tile holds at most TB blocks of max_block_bytes, far below
+    // 2^24), CPs in 24..43 and extrema in 44..63 (at most 8 per thread)
     unsigned tbytes, tcps, text;
-    const unsigned bv = (threadIdx.x < TB) ? s_bytes[threadIdx.x] : 0u;
-    const unsigned boff = cta_excl_scan<WARPS>(bv, sh.w1, &tbytes);
-    const unsigned cpo = cta_excl_scan<WARPS>((unsigned)__popc(cpm), sh.w2, &tcps);
-    const unsigned exo = cta_excl_scan<WARPS>((unsigned)__popc(exm), sh.w3, &text);
+    unsigned boff, cpo, exo;
+    {
+      const unsigned bv = (threadIdx.x < TB) ? s_bytes[threadIdx.x] : 0u;
+      const unsigned long long v = (unsigned long long)bv | ((unsigned long long)__popc(cpm) << 24) |
+                                   ((unsigned long long)__popc(exm) << 44);
+      unsigned long long tot;
+      const unsigned long long ex = cta_excl_scan64<WARPS>(v, sh.w64, &tot);
+      boff = (unsigned)(ex & 0xffffffull);
+      cpo = (unsigned)((ex >> 24) & 0xfffffull);
+      exo = (unsigned)(ex >> 44);
+      tbytes = (unsigned)(tot & 0xffffffull);
+      tcps = (unsigned)((tot >> 24) & 0xfffffull);
+      text = (unsigned)(tot >> 44);
+    }
     __syncthreads();
     if (threadIdx.x < TB) s_bytes[threadIdx.x] = boff;
     if (threadIdx.x == 0) {
