@@ -71,8 +71,8 @@ __device__ __forceinline__ unsigned compact2(unsigned x) {
 
 // 2-bit types of an octet (element t in bits 2t..2t+1); c[] holds the values
 // of the octet, nv of them valid, i0 the flat index of element 0
-__device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, long long n, long long i0,
-                                                   int nv, const float (&c)[8], const Geom &g) {
+// interior mask of an octet (bit t: element i0 + t is interior), nv valid
+__device__ __forceinline__ unsigned octet_interior(long long i0, int nv, const Geom &g) {
   // coordinates of element 0, then incremented with wrap-around
   long long r, x, y, z;
   if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
@@ -98,6 +98,19 @@ __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, 
       while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
     }
   }
+  return inter;
+}
+
+// first classification axis of an octet: planes (3D) or rows (2D)
+__device__ __forceinline__ long long octet_axis_a(const Geom &g) { return (g.nd == 2) ? g.d3 : g.plane; }
+
+// 2-bit types of an octet (element t in bits 2t..2t+1): c[] holds its values,
+// nv of them valid, i0 the flat index of element 0, inter its interior mask;
+// ma / pa hold the neighbours at -/+ octet_axis_a (loaded by the caller for
+// the interior elements, ahead of the octet's own values: the longest wait)
+__device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, long long n, long long i0,
+                                                   int nv, const float (&c)[8], const Geom &g, unsigned inter,
+                                                   const float (&ma)[8], const float (&pa)[8]) {
   if (inter == 0) return 0u;
   // +-1 neighbours: inside the octet, plus one scalar load at each end
   const float prev = (inter & 1u) ? __ldg(d + i0 - 1) : 0.f;
@@ -105,21 +118,15 @@ __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, 
 #pragma unroll
   for (int t = 0; t < 8; t++)
     if (t == nv - 1 && (inter & (1u << t))) next = __ldg(d + i0 + nv);
-  const long long o1 = (g.nd == 2) ? g.d3 : g.plane;  // first axis: rows (2D) or planes (3D)
   // Per axis, hi: c above both neighbours, lo: c below both.  c > max(m, p)
   // with a NaN-propagating max is exactly (c > m && c > p), NaNs included
   // (any NaN makes both false), and likewise for lo with min.
   unsigned hi_a = 0, lo_a = 0, hi_b = 0, lo_b = 0, hi_c = 0, lo_c = 0;
-  {
-    float m[8], p[8];
-    load_oct(d, i0 - o1, n, inter, m);
-    load_oct(d, i0 + o1, n, inter, p);
 #pragma unroll
-    for (int t = 0; t < 8; t++) {
-      if (!(inter & (1u << t))) continue;
-      if (c[t] > fmax_nan(m[t], p[t])) hi_a |= 1u << t;
-      if (c[t] < fmin_nan(m[t], p[t])) lo_a |= 1u << t;
-    }
+  for (int t = 0; t < 8; t++) {
+    if (!(inter & (1u << t))) continue;
+    if (c[t] > fmax_nan(ma[t], pa[t])) hi_a |= 1u << t;
+    if (c[t] < fmin_nan(ma[t], pa[t])) lo_a |= 1u << t;
   }
   if (g.nd == 3) {
     float m[8], p[8];
@@ -269,11 +276,19 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
         for (int t = 0; t < 8; t++) if (t < nv) q[t] = __ldg(a.ints + i0 + t);
       }
     } else {
+      unsigned inter = 0;
+      float ma[8], pa[8];
+      if (MODE == kEncClassify && nv > 0) {
+        inter = octet_interior(i0, nv, a.g);
+        const long long oa = octet_axis_a(a.g);
+        load_oct(a.data, i0 - oa, n, inter, ma);
+        load_oct(a.data, i0 + oa, n, inter, pa);
+      }
       load_oct(a.data, i0, n, nv >= 8 ? 0xffu : ((1u << nv) - 1u), x);
 #pragma unroll
       for (int t = 0; t < 8; t++) if (t < nv) q[t] = quantize(x[t], a.inv);
       if (MODE == kEncClassify) {
-        if (nv > 0) types = classify_octet(a.data, n, i0, nv, x, a.g);
+        if (nv > 0) types = classify_octet(a.data, n, i0, nv, x, a.g, inter, ma, pa);
       } else if (nv > 0) {
         if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.types + i0) & 7) == 0)) {
           const unsigned long long w = __ldg(reinterpret_cast<const unsigned long long *>(a.types + i0));
