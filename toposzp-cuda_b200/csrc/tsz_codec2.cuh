@@ -110,7 +110,8 @@ __device__ __forceinline__ long long octet_axis_a(const Geom &g) { return (g.nd 
 // the interior elements, ahead of the octet's own values: the longest wait)
 __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, long long n, long long i0,
                                                    int nv, const float (&c)[8], const Geom &g, unsigned inter,
-                                                   const float (&ma)[8], const float (&pa)[8]) {
+                                                   const float (&ma)[8], const float (&pa)[8],
+                                                   const float (&mb)[8], const float (&pb)[8]) {
   if (inter == 0) return 0u;
   // +-1 neighbours: inside the octet, plus one scalar load at each end
   const float prev = (inter & 1u) ? __ldg(d + i0 - 1) : 0.f;
@@ -129,14 +130,11 @@ __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, 
     if (c[t] < fmin_nan(ma[t], pa[t])) lo_a |= 1u << t;
   }
   if (g.nd == 3) {
-    float m[8], p[8];
-    load_oct(d, i0 - g.d3, n, inter, m);
-    load_oct(d, i0 + g.d3, n, inter, p);
 #pragma unroll
     for (int t = 0; t < 8; t++) {
       if (!(inter & (1u << t))) continue;
-      if (c[t] > fmax_nan(m[t], p[t])) hi_b |= 1u << t;
-      if (c[t] < fmin_nan(m[t], p[t])) lo_b |= 1u << t;
+      if (c[t] > fmax_nan(mb[t], pb[t])) hi_b |= 1u << t;
+      if (c[t] < fmin_nan(mb[t], pb[t])) lo_b |= 1u << t;
     }
   }
 #pragma unroll
@@ -277,18 +275,22 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
       }
     } else {
       unsigned inter = 0;
-      float ma[8], pa[8];
+      float ma[8], pa[8], mb[8], pb[8];
       if (MODE == kEncClassify && nv > 0) {
         inter = octet_interior(i0, nv, a.g);
         const long long oa = octet_axis_a(a.g);
         load_oct(a.data, i0 - oa, n, inter, ma);
         load_oct(a.data, i0 + oa, n, inter, pa);
+        if (a.g.nd == 3) {
+          load_oct(a.data, i0 - a.g.d3, n, inter, mb);
+          load_oct(a.data, i0 + a.g.d3, n, inter, pb);
+        }
       }
       load_oct(a.data, i0, n, nv >= 8 ? 0xffu : ((1u << nv) - 1u), x);
 #pragma unroll
       for (int t = 0; t < 8; t++) if (t < nv) q[t] = quantize(x[t], a.inv);
       if (MODE == kEncClassify) {
-        if (nv > 0) types = classify_octet(a.data, n, i0, nv, x, a.g, inter, ma, pa);
+        if (nv > 0) types = classify_octet(a.data, n, i0, nv, x, a.g, inter, ma, pa, mb, pb);
       } else if (nv > 0) {
         if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.types + i0) & 7) == 0)) {
           const unsigned long long w = __ldg(reinterpret_cast<const unsigned long long *>(a.types + i0));
@@ -882,8 +884,18 @@ decode2_kernel(DecArgs a) {
     }
   }
   if (TAGS && a.ext_count) {
+    // one atomic per CTA: every CTA adds to the same word, so per-warp
+    // atomics would queue at its L2 slice
+    __shared__ unsigned s_ext[kWarps];
     n_ext = __reduce_add_sync(0xffffffffu, n_ext);
-    if (lane == 0 && n_ext) atomicAdd(a.ext_count, (unsigned long long)n_ext);
+    if (lane == 0) s_ext[warp] = n_ext;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tot = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; w++) tot += s_ext[w];
+      if (tot) atomicAdd(a.ext_count, (unsigned long long)tot);
+    }
   }
 }
 
