@@ -353,3 +353,48 @@ def test_decompress_unaligned_streams(T):
     ok = ctx.decompress(topo3, sz3.topo_bytes, sort3, sz3.sort_bytes, idx3, dims, eb, 257)
     assert torch.isfinite(ok).all()
     ctx.close()
+
+
+def test_concurrent_contexts_on_host_threads(T):
+    """Workspaces are independent: host threads that each drive their own
+    context through the host-buffer calls, at the same time, get exactly the
+    bytes and fields that one thread gets alone (the first call of a fresh
+    device also uploads the post-processing weights from several threads)."""
+    import threading
+    jobs = [((40, 50, 60), "bumps", 1e-3), ((180, 360), "noise", 1e-3), ((20, 24, 28), "band", 1e-4),
+            ((96, 64, 48), "bumps", 1e-2)]
+
+    def run(job, ctx):
+        dims, kind, eb = job
+        d = field(dims, kind, 1.0, seed=11)
+        n = d.size
+        L = T.lib()
+        ht = np.empty(L.szp_b200_topo_bound(n, 64), dtype=np.uint8)
+        hs = np.empty(L.szp_b200_sort_bound(n, 64), dtype=np.uint8)
+        sz = ctx.compress_host(d, eb, 64, ht, hs)
+        out = np.empty(dims, dtype=np.float32)
+        ctx.decompress_host(ht, sz.topo_bytes, hs, sz.sort_bytes, dims, eb, 64, out, 1)
+        return ht[:sz.topo_bytes].tobytes(), hs[:sz.sort_bytes].tobytes(), out.view(np.int32).copy()
+
+    ctxs = [T.Context() for _ in jobs]
+    alone = [run(j, c) for j, c in zip(jobs, ctxs)]
+    for _ in range(2):
+        res = [None] * len(jobs)
+        errs = []
+
+        def work(i):
+            try:
+                res[i] = run(jobs[i], ctxs[i])
+            except Exception as e:
+                errs.append(e)
+        th = [threading.Thread(target=work, args=(i,)) for i in range(len(jobs))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert not errs, errs
+        for a, r in zip(alone, res):
+            assert a[0] == r[0] and a[1] == r[1]
+            assert np.array_equal(a[2], r[2])
+    for c in ctxs:
+        c.close()

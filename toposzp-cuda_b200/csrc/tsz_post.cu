@@ -80,6 +80,7 @@ struct PostArgs {
   const unsigned *L;            // lock bitmap: interior point next to an interior extremum
   const unsigned *R;            // RBF candidates (lost saddles) bitmap
   const unsigned *X;            // interior-extremum bitmap (the stencil / enforcement candidates)
+  const unsigned *XP;           // per bitmap word: list position of its first extremum (X entries before it)
   int *err;
   unsigned *restored;
 };
@@ -252,9 +253,11 @@ __device__ __forceinline__ float enforce(const PostArgs &a, const Face &f, float
 
 // Reads the face neighbours of interior point e for a stencil / enforcement
 // item.  An earlier neighbour that is a candidate of the pass (an interior
-// extremum: a bit of X) must have its result already: its S word carries the
-// value and the pass generation.  Returns false (nothing read is used) while
-// one of them is not final.  Every load is issued before the first wait.
+// extremum: a bit of X) must have its result already: the S word at its list
+// position (XP of its bitmap word plus the extrema before it in the word)
+// carries the value and the pass generation.  Returns false (nothing read is
+// used) while one of them is not final.  Every load is issued before the
+// first wait.
 template <int ND>
 __device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &f) {
   const long long pl = a.g.plane, d3 = a.g.d3;
@@ -262,8 +265,18 @@ __device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &
   // so each lies in the field
   const long long qb[3] = {e - pl, e - d3, e - 1};
   bool cb[3];
+  unsigned pos[3];
 #pragma unroll
-  for (int k = 0; k < 3; k++) cb[k] = (ND == 3 || k > 0) && bit_at(a.X, qb[k]);
+  for (int k = 0; k < 3; k++) {
+    cb[k] = false;
+    pos[k] = 0;
+    if (ND == 2 && k == 0) continue;
+    const long long wi = qb[k] >> 5;
+    const unsigned bw = a.X[wi], base = a.XP[wi];
+    const unsigned b = (unsigned)(qb[k] & 31);
+    cb[k] = (bw >> b) & 1u;
+    pos[k] = base + (unsigned)__popc(bw & ((1u << b) - 1u));
+  }
   unsigned long long wb[3];
   float fb[3];
 #pragma unroll
@@ -271,7 +284,7 @@ __device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &
     wb[k] = 0;
     fb[k] = 0.f;
     if (ND == 2 && k == 0) continue;
-    if (cb[k]) wb[k] = ld_rlx(&a.S[qb[k]]);
+    if (cb[k]) wb[k] = ld_rlx(&a.S[pos[k]]);
     else fb[k] = a.F[qb[k]];
   }
   f.xp = (ND == 3) ? a.F[e + pl] : 0.f;
@@ -623,7 +636,8 @@ constexpr int kListTile = kPostThreads * kListPer;
 __global__ void __launch_bounds__(kPostThreads)
 list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, TileDesc *desc, unsigned *tile_ctr,
                   int *err, unsigned *X, unsigned *Z, unsigned char *Eb, unsigned char *Ib,
-                  unsigned long long *tot, const float *__restrict__ O, float *OX, float *OZ) {
+                  unsigned long long *tot, const float *__restrict__ O, float *OX, float *OZ,
+                  unsigned *XP) {
   __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
   __shared__ unsigned s_buf[kListTile];
   __shared__ long long s_tile;
@@ -713,6 +727,8 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
     }
     __syncthreads();
     const unsigned long long xb = s_xb, zb = s_zb;
+    // list position of the first extremum of this thread's bitmap word
+    if (i0 < n) XP[i0 >> 5] = (unsigned)(xb + eo);
     for (unsigned k = threadIdx.x; k < te; k += kPostThreads) {
       const unsigned q = s_buf[k];
       X[xb + k] = q;
@@ -777,9 +793,12 @@ __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__r
   }
   if (ok) atomicAdd(a.restored, 1u);
   // in place: every reader of e's pre-pass value has finished (they are the
-  // earlier candidates e waited for); later readers take e's result from S
+  // earlier candidates e waited for); later readers take e's result from S,
+  // at e's list position for the stencil / enforcement passes (dense, one
+  // coalesced word per item), at e itself for the RBF / axis passes
   a.F[e] = r;
-  st_rlx(&a.S[e], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
+  const long long sp = (PASS == kPassStencil || PASS == kPassEnforce) ? (long long)idx : e;
+  st_rlx(&a.S[sp], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
   return false;
 }
 
@@ -1014,9 +1033,9 @@ static cudaError_t upload_weights(int dev) {
 size_t post_scratch_bytes(unsigned long long n) {
   const unsigned long long ntiles = (n + kPostTile - 1) / kPostTile;
   const unsigned long long words = (n + 31) / 32;
-  // T, descriptors, lock + RBF + extrema + interior bitmaps, lists X and Z,
-  // worklists (2), Y, raw values of X and Z
-  return a256(n) + a256((ntiles + 1) * sizeof(TileDesc)) + 4 * a256(words * 4 + 4) + 7 * a256(n * 4) + 8192;
+  // T, descriptors, lock + RBF + extrema + interior bitmaps + extremum word
+  // positions, lists X and Z, worklists (2), Y, raw values of X and Z
+  return a256(n) + a256((ntiles + 1) * sizeof(TileDesc)) + 5 * a256(words * 4 + 4) + 7 * a256(n * 4) + 8192;
 }
 
 
@@ -1247,8 +1266,9 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   unsigned *W0 = A.take<unsigned>(n), *W1 = A.take<unsigned>(n);
   unsigned *R = A.take<unsigned>((n + 31) / 32);
   unsigned *Eb = A.take<unsigned>((n + 31) / 32 + 1), *Ib = A.take<unsigned>((n + 31) / 32 + 1);
+  unsigned *XP = A.take<unsigned>((n + 31) / 32 + 1);
   float *OX = A.take<float>(n), *OZ = A.take<float>(n);
-  if (!X || !Z || !Y || !W0 || !W1 || !R || !Eb || !Ib || !OX || !OZ) {
+  if (!X || !Z || !Y || !W0 || !W1 || !R || !Eb || !Ib || !XP || !OX || !OZ) {
     set_error("scratch arena too small for post-processing");
     return -1;
   }
@@ -1270,7 +1290,7 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
     const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 4);
     list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
                                                     Z, reinterpret_cast<unsigned char *>(Eb),
-                                                    reinterpret_cast<unsigned char *>(Ib), d_tot, d_orig, OX, OZ);
+                                                    reinterpret_cast<unsigned char *>(Ib), d_tot, d_orig, OX, OZ, XP);
   }
   ctx->launches += 1;
   unsigned long long tot = 0;
@@ -1290,6 +1310,7 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   a.eb = eb;
   a.eps = fmaxf(1e-6f, 0.1f * eb);
   a.S = d_S;
+  a.XP = XP;
   a.err = reinterpret_cast<int *>(w + 4);
   a.restored = reinterpret_cast<unsigned *>(w + 5);
   const int rc = (g.nd == 2)
