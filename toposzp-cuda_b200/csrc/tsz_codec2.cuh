@@ -354,7 +354,7 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
       tcps = (unsigned)((tot >> 24) & 0xfffffull);
       text = (unsigned)(tot >> 44);
     }
-    __syncthreads();
+    // each thread overwrites only the entry it read before the scan
     if (threadIdx.x < TB) s_bytes[threadIdx.x] = boff;
     if (threadIdx.x == 0) {
       sh.tile_bytes = tbytes;
