@@ -729,15 +729,41 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
     const unsigned long long xb = s_xb, zb = s_zb;
     // list position of the first extremum of this thread's bitmap word
     if (i0 < n) XP[i0 >> 5] = (unsigned)(xb + eo);
-    for (unsigned k = threadIdx.x; k < te; k += kPostThreads) {
-      const unsigned q = s_buf[k];
-      X[xb + k] = q;
-      OX[xb + k] = O[q];
+    // entries four at a time per thread: the raw-value gathers of a batch
+    // are in flight together
+    for (unsigned k0 = threadIdx.x; k0 < te; k0 += 4 * kPostThreads) {
+      unsigned q[4];
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const unsigned k = k0 + u * kPostThreads;
+        q[u] = k < te ? s_buf[k] : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (k0 + u * kPostThreads < te) v[u] = O[q[u]];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const unsigned k = k0 + u * kPostThreads;
+        if (k < te) { X[xb + k] = q[u]; OX[xb + k] = v[u]; }
+      }
     }
-    for (unsigned k = threadIdx.x; k < ts; k += kPostThreads) {
-      const unsigned q = s_buf[kListTile - 1 - k];
-      Z[zb + k] = q;
-      OZ[zb + k] = O[q];
+    for (unsigned k0 = threadIdx.x; k0 < ts; k0 += 4 * kPostThreads) {
+      unsigned q[4];
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const unsigned k = k0 + u * kPostThreads;
+        q[u] = k < ts ? s_buf[kListTile - 1 - k] : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (k0 + u * kPostThreads < ts) v[u] = O[q[u]];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const unsigned k = k0 + u * kPostThreads;
+        if (k < ts) { Z[zb + k] = q[u]; OZ[zb + k] = v[u]; }
+      }
     }
     __syncthreads();
   }
@@ -1287,7 +1313,7 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   const long long ltiles = (n + kListTile - 1) / kListTile;
   if (cuda_fail(cudaMemsetAsync(desc, 0, (ltiles + 1) * sizeof(TileDesc), s), "memset")) return -1;
   {
-    const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 4);
+    const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 6);
     list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
                                                     Z, reinterpret_cast<unsigned char *>(Eb),
                                                     reinterpret_cast<unsigned char *>(Ib), d_tot, d_orig, OX, OZ, XP);
