@@ -1313,7 +1313,7 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   const long long ltiles = (n + kListTile - 1) / kListTile;
   if (cuda_fail(cudaMemsetAsync(desc, 0, (ltiles + 1) * sizeof(TileDesc), s), "memset")) return -1;
   {
-    const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 6);
+    const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 4);
     list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
                                                     Z, reinterpret_cast<unsigned char *>(Eb),
                                                     reinterpret_cast<unsigned char *>(Ib), d_tot, d_orig, OX, OZ, XP);
