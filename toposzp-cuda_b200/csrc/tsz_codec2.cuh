@@ -694,8 +694,9 @@ __device__ __forceinline__ unsigned long long ld_bytes8(const unsigned char *img
   return ((unsigned long long)hi << 32) | lo;
 }
 
+// eight CTAs per SM (32 registers, full occupancy)
 template <bool TAGS, int G>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 8)
 decode2_kernel(DecArgs a) {
   constexpr int BPW = 32 / G;
   constexpr int TB = kWarps * BPW;

@@ -852,8 +852,10 @@ __device__ __forceinline__ bool pass_item_local(const PostArgs &a, const unsigne
 
 // One round of a pass over a worklist of list indices (identity when W is
 // null).  Items whose earlier candidates are not final yet go to Wn.
+// eight CTAs per SM (32 registers): the round is latency-bound, more warps
+// hide more of it
 template <int PASS, int ND>
-__global__ void __launch_bounds__(kPostThreads)
+__global__ void __launch_bounds__(kPostThreads, 8)
 pass_round_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *__restrict__ W,
                   unsigned nw, unsigned *__restrict__ Wn, unsigned *wn_count) {
   const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
