@@ -834,7 +834,7 @@ __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__r
 // few times, a block barrier apart, so that chains inside the CTA resolve in
 // this round.  Every thread of the CTA must call it.  Returns true while the
 // item is still pending.
-constexpr int kLocalRetries = 4;
+constexpr int kLocalRetries = 5;
 
 template <int PASS, int ND>
 __device__ __forceinline__ bool pass_item_local(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx,
