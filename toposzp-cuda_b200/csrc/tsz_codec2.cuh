@@ -244,11 +244,9 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
   const int warp = threadIdx.x >> 5;
   const int gi = lane / G, l = lane % G;
   const bool tags = (MODE != kEncInts);
-  uint32_t *imgw = reinterpret_cast<uint32_t *>(img);
   const long long n = (long long)a.n;
   const int B = a.B;
   const long long nblocks = (n + B - 1) / B;
-  const long long ntiles = (nblocks + TB - 1) / TB;
   {
     const int bi = warp * BPW + gi;
     const long long blk = tile * TB + bi;
@@ -363,7 +361,6 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
       publish_aggregate(a.desc, tile, tbytes, ((unsigned long long)tcps << 32) | text);
     }
     __syncthreads();
-    const unsigned tile_bytes = sh.tile_bytes;
     // critical-point pairs of the tile, staged in thread (= raster) order;
     // extremum indices tile-local until the look-back gives the base
     uint2 *cp_stage = reinterpret_cast<uint2 *>(img + enc2_img_bytes(B, tags, TB));
