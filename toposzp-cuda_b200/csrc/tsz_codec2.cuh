@@ -160,30 +160,6 @@ __device__ __forceinline__ unsigned classify_octet(const float *__restrict__ d, 
   return spread2(mx | sd) | (spread2(mn | sd) << 1);
 }
 
-// CTA-wide exclusive scan of one value per thread (WARPS warps);
-// returns the exclusive prefix and writes the total to *total
-template <int WARPS = kWarps>
-__device__ __forceinline__ unsigned cta_excl_scan(unsigned v, unsigned *s_warp, unsigned *total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned inc = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += u;
-  }
-  if (lane == 31) s_warp[warp] = inc;
-  __syncthreads();
-  unsigned wpre = 0, tot = 0;
-#pragma unroll
-  for (int w = 0; w < WARPS; w++) {
-    const unsigned sw = s_warp[w];
-    if (w < warp) wpre += sw;
-    tot += sw;
-  }
-  *total = tot;
-  return wpre + inc - v;
-}
-
 // CTA-wide exclusive scan of one 64-bit value per thread (packed fields that
 // never carry into each other); returns the exclusive prefix, total in *total
 template <int WARPS>

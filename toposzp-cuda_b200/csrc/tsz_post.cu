@@ -110,7 +110,6 @@ __device__ __forceinline__ bool interior(const Geom &g, const C3 &c) {
   if (g.nd == 3 && (c.x < 1 || c.x > g.d1 - 2)) return false;
   return true;
 }
-__device__ __forceinline__ bool interior_at(const Geom &g, long long q) { return interior(g, coords(g, q)); }
 
 // 4/6-neighbour classification on F (stable during a pass)
 __device__ __forceinline__ int classify_F(const PostArgs &a, long long q) {
@@ -521,104 +520,6 @@ __device__ float axis3(const PostArgs &a, long long e, const C3 &c, float o, boo
 // ----------------------------------------------------------------------------
 // candidate lists
 // ----------------------------------------------------------------------------
-
-// Interior extrema (list X) and interior saddles (list Z), both in raster
-// order, from the types array: per-tile counts, a scan over the tiles, then a
-// second pass that writes the positions.  Tiles of kPostTile points, 8 per
-// thread; counts packed as (extrema << 32) | saddles.
-__device__ __forceinline__ void tile_masks(const unsigned char *__restrict__ T, const Geom &g, long long n,
-                                           long long i0, unsigned &em, unsigned &sm) {
-  em = 0;
-  sm = 0;
-  if (i0 >= n) return;
-  long long r, x, y, z;
-  if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
-  else { x = fdivmod(i0, g.plane, g.m_plane, r); y = fdivmod(r, g.d3, g.m_d3, z); }
-  unsigned long long w = 0;
-  if (i0 + 8 <= n && ((reinterpret_cast<uintptr_t>(T + i0) & 7) == 0)) {
-    w = *reinterpret_cast<const unsigned long long *>(T + i0);
-  } else {
-    for (int u = 0; u < 8; u++) if (i0 + u < n) w |= (unsigned long long)T[i0 + u] << (8 * u);
-  }
-  if (w == 0) return;
-  for (int u = 0; u < kPostPer; u++) {
-    if (i0 + u >= n) break;
-    bool in = y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
-    if (g.nd == 3) in = in && x >= 1 && x <= g.d1 - 2;
-    const unsigned t = (unsigned)(w >> (8 * u)) & 3u;
-    if (in && (t == 1u || t == 2u)) em |= 1u << u;
-    if (in && t == 3u) sm |= 1u << u;
-    z++;
-    while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
-  }
-}
-
-__global__ void __launch_bounds__(kPostThreads)
-list_count_kernel(const unsigned char *__restrict__ T, Geom g, long long n, unsigned long long *cnt) {
-  __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
-  const long long i0 = (long long)blockIdx.x * kPostTile + (long long)threadIdx.x * kPostPer;
-  unsigned em, sm;
-  tile_masks(T, g, n, i0, em, sm);
-  unsigned te, ts;
-  cta_excl_scan_post((unsigned)__popc(em), s_w1, &te);
-  cta_excl_scan_post((unsigned)__popc(sm), s_w2, &ts);
-  if (threadIdx.x == 0) cnt[blockIdx.x] = ((unsigned long long)te << 32) | ts;
-}
-
-// exclusive scan of packed tile counts (one CTA of 1024 threads); totals at cnt[ntiles]
-__global__ void list_scan_kernel(unsigned long long *cnt, long long ntiles) {
-  __shared__ unsigned long long part[1024];
-  const long long per = (ntiles + blockDim.x - 1) / blockDim.x;
-  const long long i0 = threadIdx.x * per;
-  unsigned long long sum = 0;
-  for (long long i = 0; i < per; i++) if (i0 + i < ntiles) sum += cnt[i0 + i];
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-    const unsigned long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0ull;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
-  }
-  unsigned long long run = part[threadIdx.x] - sum;
-  for (long long i = 0; i < per; i++)
-    if (i0 + i < ntiles) { const unsigned long long v = cnt[i0 + i]; cnt[i0 + i] = run; run += v; }
-  if (threadIdx.x == blockDim.x - 1) cnt[ntiles] = part[threadIdx.x];
-}
-
-__global__ void __launch_bounds__(kPostThreads)
-list_write_kernel(const unsigned char *__restrict__ T, Geom g, long long n, const unsigned long long *cnt,
-                  unsigned *X, unsigned *Z, unsigned char *Eb, unsigned char *Ib) {
-  __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
-  const long long i0 = (long long)blockIdx.x * kPostTile + (long long)threadIdx.x * kPostPer;
-  unsigned em, sm;
-  tile_masks(T, g, n, i0, em, sm);
-  if (i0 < n) {
-    // interior bits of the 8 points (byte of the interior bitmap)
-    unsigned im = 0;
-    long long r, x, y, z;
-    if (g.nd == 2) { x = 0; y = fdivmod(i0, g.d3, g.m_d3, r); z = r; }
-    else { x = fdivmod(i0, g.plane, g.m_plane, r); y = fdivmod(r, g.d3, g.m_d3, z); }
-    for (int u = 0; u < kPostPer && i0 + u < n; u++) {
-      bool in = y >= 1 && y <= g.d2 - 2 && z >= 1 && z <= g.d3 - 2;
-      if (g.nd == 3) in = in && x >= 1 && x <= g.d1 - 2;
-      if (in) im |= 1u << u;
-      z++;
-      while (z >= g.d3) { z -= g.d3; y++; if (y >= g.d2) { y -= g.d2; x++; } }
-    }
-    Eb[i0 >> 3] = (unsigned char)em;
-    Ib[i0 >> 3] = (unsigned char)im;
-  }
-  unsigned te, ts;
-  const unsigned eo = cta_excl_scan_post((unsigned)__popc(em), s_w1, &te);
-  const unsigned so = cta_excl_scan_post((unsigned)__popc(sm), s_w2, &ts);
-  const unsigned long long base = cnt[blockIdx.x];
-  unsigned long long xe = (base >> 32) + eo, xs = (base & 0xffffffffull) + so;
-  for (int u = 0; u < kPostPer; u++) {
-    if (em & (1u << u)) X[xe++] = (unsigned)(i0 + u);
-    if (sm & (1u << u)) Z[xs++] = (unsigned)(i0 + u);
-  }
-}
 
 // Interior extrema (X) and interior saddles (Z) in raster order plus the two
 // bitmaps (extrema Eb, interior Ib), in one pass over the types: persistent
@@ -1302,7 +1203,6 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   }
   unsigned long long *w = ctx->d_words;  // [9] pass status, [10] round counters
   if (cuda_fail(cudaMemsetAsync(w, 0, 96, s), "memset")) return -1;
-  const long long ntiles = (n + kPostTile - 1) / kPostTile;
   {
     // the words past the last written byte of the two bitmaps must read as zero
     const long long words = (n + 31) / 32;
