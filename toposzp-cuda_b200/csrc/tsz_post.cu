@@ -646,7 +646,11 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const unsigned k = k0 + u * kPostThreads;
-        if (k < te) { X[xb + k] = q[u]; OX[xb + k] = v[u]; }
+        if (k < te) {
+          // a list position past n means corrupt tile offsets: recorded, not written
+          if (xb + k < (unsigned long long)n) { X[xb + k] = q[u]; OX[xb + k] = v[u]; }
+          else atomicExch(err, kErrMalformed);
+        }
       }
     }
     for (unsigned k0 = threadIdx.x; k0 < ts; k0 += 4 * kPostThreads) {
@@ -663,7 +667,10 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const unsigned k = k0 + u * kPostThreads;
-        if (k < ts) { Z[zb + k] = q[u]; OZ[zb + k] = v[u]; }
+        if (k < ts) {
+          if (zb + k < (unsigned long long)n) { Z[zb + k] = q[u]; OZ[zb + k] = v[u]; }
+          else atomicExch(err, kErrMalformed);
+        }
       }
     }
     __syncthreads();
@@ -1215,7 +1222,7 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   const long long ltiles = (n + kListTile - 1) / kListTile;
   if (cuda_fail(cudaMemsetAsync(desc, 0, (ltiles + 1) * sizeof(TileDesc), s), "memset")) return -1;
   {
-    const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 4);
+    const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 6);
     list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
                                                     Z, reinterpret_cast<unsigned char *>(Eb),
                                                     reinterpret_cast<unsigned char *>(Ib), d_tot, d_orig, OX, OZ, XP);
