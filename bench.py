@@ -519,7 +519,12 @@ def e2e_pipelined(T, f, dims, eb, B, steps, out, world, streams=2):
         h_out = torch.empty(dims, dtype=torch.float32).pin_memory()
         workers.append({"bufs": (h_field, h_topo, h_sort, h_out), "ctx": T.Context(), "err": None})
 
+    dev = out.device
+
     def run(w, k, start):
+        # a new host thread starts on device 0: select this rank's device,
+        # on which the workspaces were created
+        torch.cuda.set_device(dev)
         hf, ht, hs, ho = (x.numpy() for x in w["bufs"])
         start.wait()
         try:
