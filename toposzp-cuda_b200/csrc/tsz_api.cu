@@ -735,6 +735,7 @@ int szp_b200_topo_compress_dev(szp_b200_ctx *ctx, const float *d_data, szp_b200_
                                unsigned char *d_sort, uint64_t *d_blk_index,
                                szp_b200_sizes *sizes) {
   clear_error();
+  DeviceGuard dg(ctx);
   return compress_dev_impl(ctx, d_data, geom, absErrBound, blockSize, d_topo, d_sort, d_blk_index, sizes, nullptr,
                            0);
 }
@@ -861,6 +862,7 @@ int szp_b200_topo_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_topo,
                                  int blockSize, float *d_out, unsigned char *d_types,
                                  int postprocess) {
   clear_error();
+  DeviceGuard dg(ctx);
   return decompress_dev_impl(ctx, d_topo, topo_bytes, d_sort, sort_bytes, d_blk_index, geom, absErrBound,
                              blockSize, d_out, d_types, postprocess, false, nullptr);
 }
@@ -869,6 +871,7 @@ int szp_b200_topo_postprocess_dev(szp_b200_ctx *ctx, float *d_data, const float 
                                   const int *d_types, const int *d_sp, size_t n_sp,
                                   szp_b200_geom geom, float absErrBound, int axis_stencil) {
   clear_error();
+  DeviceGuard dg(ctx);
   if (!ctx || !d_data || !d_orig || !d_types) { set_error("null argument"); return -1; }
   unsigned long long n;
   Geom g;
@@ -958,6 +961,7 @@ int szp_b200_topo_compress_host(szp_b200_ctx *ctx, const float *h_data, szp_b200
                                 size_t topo_cap, unsigned char *h_sort, size_t sort_cap,
                                 szp_b200_sizes *sizes) {
   clear_error();
+  DeviceGuard dg(ctx);
   if (!ctx || !h_data || !h_topo || !h_sort || !sizes) { set_error("null argument"); return -1; }
   if (!check_block_size(blockSize, "szp_b200_topo_compress_host")) return -1;
   unsigned long long n;
@@ -1074,6 +1078,7 @@ int szp_b200_topo_decompress_host(szp_b200_ctx *ctx, const unsigned char *h_topo
                                   const unsigned char *h_sort, size_t sort_bytes, szp_b200_geom geom,
                                   float absErrBound, int blockSize, float *h_out, int postprocess) {
   clear_error();
+  DeviceGuard dg(ctx);
   if (!ctx || !h_topo || !h_out) { set_error("null argument"); return -1; }
   if (!check_block_size(blockSize, "szp_b200_topo_decompress_host")) return -1;
   unsigned long long n;

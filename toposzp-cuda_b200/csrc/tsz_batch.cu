@@ -743,6 +743,7 @@ int szp_b200_batch_tuning(szp_b200_batch *b, int *shape, float *ms, int max) {
 szp_b200_ctx *szp_b200_batch_ctx(szp_b200_batch *b) { return b ? b->ctx : nullptr; }
 
 int szp_b200_batch_compress(szp_b200_batch *b, szp_b200_batch_field *fs, int count) {
+  DeviceGuard dg(b ? b->ctx : nullptr);
   clear_error();
   if (!b || (!fs && count)) { set_error("null argument"); return -1; }
   if (count <= 0) return 0;

@@ -173,6 +173,7 @@ szp_b200_ctx *szp_b200_ctx_create(void *cuda_stream) {
 }
 
 void szp_b200_ctx_destroy(szp_b200_ctx *ctx) {
+  tsz::DeviceGuard dg(ctx);
   if (!ctx) return;
   tsz::ctx_free(ctx);
   delete ctx;

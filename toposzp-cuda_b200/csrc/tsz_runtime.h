@@ -61,6 +61,25 @@ struct szp_b200_ctx {
 };
 
 namespace tsz {
+// Makes the workspace's device current for the duration of a call (a thread
+// other than the one that created the workspace may start on another
+// device) and restores the caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(const szp_b200_ctx *ctx) {
+    int cur = 0;
+    if (ctx && cudaGetDevice(&cur) == cudaSuccess && cur != ctx->device && cudaSetDevice(ctx->device) == cudaSuccess)
+      prev = cur;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+}  // namespace tsz
+
+namespace tsz {
 
 // Per-thread default workspace used by the reference-compatible entry points.
 szp_b200_ctx *default_ctx();
