@@ -227,6 +227,7 @@ def cpu_port_run(field: np.ndarray, eb: float, B: int):
 
 def reference_leg(f, planes, threads):
     import oracle as O
+    planes = min(planes, f.dims[0])
     sample = np.ascontiguousarray(f.data[:planes])
     eb = f.abs_eb()
     kind = "reference" if O.ref_available() else "port"
@@ -473,7 +474,7 @@ def run_reference_arm(args):
     # each step is a bounded sample of the field: 128 planes (33.5 M elements,
     # far larger than the host caches, so the rate stands for the whole field)
     # for up to 20 steps, fewer planes per step for more steps (about 100 s in all)
-    planes = int(min(args.cpu_planes, 128, max(32, 2560 // max(1, args.steps))))
+    planes = int(min(args.cpu_planes, 128, max(32, 2560 // max(1, args.steps)), f.dims[0]))
     for _ in range(args.warmup):
         reference_leg(f, 4, threads)
     vals, info = [], None
