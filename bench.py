@@ -205,7 +205,15 @@ def cpu_reference_run(field: np.ndarray, eb: float, B: int, threads: int):
     d = np.ascontiguousarray(field, dtype=np.float32)
     t0 = time.perf_counter()
     cp = O.ref_sort_cp(O.ref_find_cp(d, eb), d)
+    # The reference's sort-position compressor frees its per-thread offset
+    # table inside `omp single` with no barrier before it, while other threads
+    # may still copy with it (SZp/src/szp_topology_3d.cc:405-416,
+    # SZp/src/szp_float.cc:850-864): a use after free that crashes now and
+    # then with several threads.  That call (a small share of the work) runs on
+    # one thread; every other call uses all of them.
+    O.set_ref_threads(1)
     sp_stream = O.ref_compress_sp(cp, B)
+    O.set_ref_threads(threads)
     topo = O.ref_compress_topo(d, eb, B, cp)
     raw, fn = O.ref_decompress_topo(topo, d.size, eb, B)
     e = int(np.count_nonzero((cp["type"] == 1) | (cp["type"] == 2)))

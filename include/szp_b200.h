@@ -202,6 +202,36 @@ SZP_B200_API int szp_b200_topo_postprocess_dev(szp_b200_ctx *ctx, float *d_data,
                                   const int *d_types, const int *d_sp, size_t n_sp,
                                   szp_b200_geom geom, float absErrBound, int axis_stencil);
 
+/* Topology report of a decompressed field against the original (device
+ * pointers, both float[n]); the counts of the reference drivers' checks
+ * (example/test_cuda_topology.cu:540-602, 636-660, 800-868 and
+ * example/test_cuda_topology_3d.cu:636-730).  A critical point is
+ * preserved when the decompressed field classifies the same point with the
+ * same type; lost when it is a regular point there; changed otherwise; new
+ * when the decompressed field has a critical point where the original has
+ * none.  pairs / violations: adjacent interior pairs (+1 along each axis,
+ * both points interior) whose original values differ, and those whose order
+ * changed; [0] all, [1] at least one critical point, [2] both critical
+ * points, [3] at least one extremum.  The reference accepts a run at
+ * max_err <= 2 eb with more than 90 % of the critical points preserved.
+ * Arrays indexed by type hold the total at [0] and type t at [t]. */
+typedef struct {
+    uint64_t orig_cps[4];
+    uint64_t dec_cps[4];
+    uint64_t preserved, lost, changed, new_cps;
+    uint64_t lost_by_type[4];
+    uint64_t pairs[4];
+    uint64_t violations[4];
+    uint64_t over_1eb;      /* |error| > 1.01 eb */
+    uint64_t over_2eb;      /* |error| > 2 eb */
+    double max_err;
+} szp_b200_topo_report;
+
+/* Synchronous on the workspace stream.  Returns 0 on success. */
+SZP_B200_API int szp_b200_topo_check(szp_b200_ctx *ctx, const float *d_orig, const float *d_dec,
+                                     szp_b200_geom geom, float absErrBound,
+                                     szp_b200_topo_report *report);
+
 /* ------------------------------------------------------------------ */
 /* Batched compression (no reference counterpart)                      */
 /* ------------------------------------------------------------------ */

@@ -360,3 +360,87 @@ def ref_post(data, orig, fn, sp, eb: float, axis_stencil=False):
         if axis_stencil:
             rest += L.ref3d_axis_saddles(_p(d), _p(t), _p(o), a, b, c, eb)
     return d, rest
+
+
+# ---------------------------------------------------------------------------
+# topology report (restates the reference drivers' verification steps)
+# ---------------------------------------------------------------------------
+
+def _classify(f: np.ndarray) -> np.ndarray:
+    """Types of every point (0 on the boundary): 4-neighbour in 2D
+    (SZp/src/szp_cuda_topology.cu:57-64), 6-neighbour in 3D
+    (example/test_cuda_topology_3d.cu:52-73)."""
+    f = f32(f)
+    t = np.zeros(f.shape, dtype=np.int8)
+    inner = tuple(slice(1, -1) for _ in f.shape)
+    c = f[inner]
+    hi, lo = [], []
+    for ax in range(f.ndim):
+        m = [slice(1, -1)] * f.ndim
+        p = [slice(1, -1)] * f.ndim
+        m[ax] = slice(0, -2)
+        p[ax] = slice(2, None)
+        a, b = f[tuple(m)], f[tuple(p)]
+        hi.append((c > a) & (c > b))
+        lo.append((c < a) & (c < b))
+    if f.ndim == 2:
+        mx = hi[0] & hi[1]
+        mn = lo[0] & lo[1] & ~mx
+        sd = ((lo[0] & hi[1]) | (hi[0] & lo[1])) & ~mx & ~mn
+    else:
+        mx = hi[0] & hi[1] & hi[2]
+        mn = lo[0] & lo[1] & lo[2] & ~mx
+        sd = (hi[0] | hi[1] | hi[2]) & (lo[0] | lo[1] | lo[2]) & ~mx & ~mn
+    ti = np.zeros(c.shape, dtype=np.int8)
+    ti[mx] = 1
+    ti[mn] = 2
+    ti[sd] = 3
+    t[inner] = ti
+    return t
+
+
+def topo_report(orig: np.ndarray, dec: np.ndarray, eb: float) -> dict:
+    """Critical-point preservation, error bound and local order of a
+    decompressed field (example/test_cuda_topology.cu:540-602, 636-660,
+    800-868; example/test_cuda_topology_3d.cu:636-730; the order check is
+    applied to every axis in 3D)."""
+    o, d = f32(orig), f32(dec)
+    to, td = _classify(o), _classify(d)
+    r = {}
+    r["orig_cps"] = [int(np.count_nonzero(to))] + [int(np.count_nonzero(to == k)) for k in (1, 2, 3)]
+    r["dec_cps"] = [int(np.count_nonzero(td))] + [int(np.count_nonzero(td == k)) for k in (1, 2, 3)]
+    cp = to != 0
+    r["preserved"] = int(np.count_nonzero(cp & (td == to)))
+    lost = cp & (td == 0)
+    r["lost"] = int(np.count_nonzero(lost))
+    r["changed"] = int(np.count_nonzero(cp & (td != 0) & (td != to)))
+    r["new_cps"] = int(np.count_nonzero((td != 0) & ~cp))
+    r["lost_by_type"] = [0] + [int(np.count_nonzero(lost & (to == k))) for k in (1, 2, 3)]
+    err = np.abs(o.astype(np.float64) - d.astype(np.float64))
+    ok = ~np.isnan(err)
+    r["max_err"] = float(err[ok].max()) if ok.any() else 0.0
+    r["over_1eb"] = int(np.count_nonzero(err > float(eb) * 1.01))
+    r["over_2eb"] = int(np.count_nonzero(err > float(eb) * 2.0))
+    pairs, viol = [0] * 4, [0] * 4
+    inner = tuple(slice(1, -1) for _ in o.shape)
+    for ax in range(o.ndim):
+        # a interior, b = a + 1 along ax, b interior too
+        sa = list(inner)
+        sb = list(inner)
+        sa[ax] = slice(1, -2)
+        sb[ax] = slice(2, -1)
+        sa, sb = tuple(sa), tuple(sb)
+        oo = np.sign(o[sa].astype(np.float64) - o[sb].astype(np.float64))
+        do = np.sign(d[sa].astype(np.float64) - d[sb].astype(np.float64))
+        oo = np.where(np.isnan(oo), 0, oo)
+        do = np.where(np.isnan(do), 0, do)
+        keep = oo != 0
+        v = keep & (oo != do)
+        ta, tb = to[sa], to[sb]
+        cats = [np.ones_like(keep), (ta != 0) | (tb != 0), (ta != 0) & (tb != 0),
+                (ta == 1) | (ta == 2) | (tb == 1) | (tb == 2)]
+        for k, m in enumerate(cats):
+            pairs[k] += int(np.count_nonzero(keep & m))
+            viol[k] += int(np.count_nonzero(v & m))
+    r["pairs"], r["violations"] = pairs, viol
+    return r

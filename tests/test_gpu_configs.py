@@ -1,0 +1,132 @@
+"""Bit-exact parity at the full sizes of the benchmark workloads.
+
+tests/golden/configs.json holds SHA-256 digests of the reference's own CPU
+library and driver post-processing (built from the reference sources, one
+OpenMP thread) on these workloads, made by tests/golden/make_config_golden.py:
+
+  c1  2D 1800x3600 bump field, abs eb 1e-3      (also compared byte for byte with the oracle)
+  c2  3D 100x500x500 bump field, rel eb 1e-4    (also compared byte for byte with the oracle)
+  c3  3D 512^3 band-limited field, abs eb 1e-4  (34.5 M critical points)
+  c4  the 256-field mixed batch                  (per-field streams of one batched call)
+
+Each single-field workload goes through the fused device path (streams, raw
+decode with the device block parser, tags, post-processed field), the
+reference entry points (critical-point list, sorted), and the topology report
+(the reference drivers' acceptance rule: max error <= 2 eb, more than 90 % of
+the critical points preserved)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import synth
+
+pytestmark = pytest.mark.gpu
+
+GOLD_PATH = os.path.join(os.path.dirname(__file__), "golden", "configs.json")
+
+
+def gold():
+    with open(GOLD_PATH) as fh:
+        return json.load(fh)
+
+
+def digest(b):
+    return hashlib.sha256(b).hexdigest()
+
+
+@pytest.fixture(scope="module")
+def T(ora):
+    import torch
+    import toposzp_b200
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    toposzp_b200.lib()
+    return toposzp_b200
+
+
+def _single(T, ora, f, g, with_oracle):
+    import torch
+    d, dims, B = f.data, f.dims, f.block_size
+    eb = f.abs_eb()
+    assert digest(d.tobytes()) == g["field"], "input field differs from the one the digests were made on"
+    assert np.float32(eb) == np.float32(g["abs_eb"])
+    ctx = T.Context()
+    dd = torch.from_numpy(d.reshape(-1).copy()).cuda()
+    topo, sort, idx, sizes = ctx.compress(dd, dims, eb, B)
+    assert (sizes.cp_count, sizes.extrema_count) == (g["cp_count"], g["extrema"])
+    topo_b = topo[: sizes.topo_bytes].cpu().numpy().tobytes()
+    sort_b = sort[: sizes.sort_bytes].cpu().numpy().tobytes()
+    assert sizes.topo_bytes == g["topo_bytes"] and digest(topo_b) == g["topo"]
+    if g["sort"] is not None:
+        assert sizes.sort_bytes == g["sort_bytes"] and digest(sort_b) == g["sort"]
+    # raw decode through the device block parser (no index), tags as bytes
+    tys = torch.empty(d.size, dtype=torch.uint8, device="cuda")
+    raw = ctx.decompress(topo, sizes.topo_bytes, sort, sizes.sort_bytes, None, dims, eb, B,
+                         postprocess=0, types=tys)
+    raw_h = raw.cpu().numpy()
+    assert digest(raw_h.tobytes()) == g["raw"]
+    assert digest(tys.cpu().numpy().tobytes()) == g["types"]
+    # decode + post-processing (stencils, enforcement, RBF), with the block index
+    post = ctx.decompress(topo, sizes.topo_bytes, sort, sizes.sort_bytes, idx, dims, eb, B, postprocess=1)
+    post_h = post.cpu().numpy()
+    assert digest(post_h.tobytes()) == g["post"]
+    rep = ctx.topo_check(dd, post, dims, eb)
+    assert rep["max_err"] <= 2.0 * eb and rep["over_2eb"] == 0
+    assert rep["preserved"] > 0.9 * rep["orig_cps"][0]
+    assert rep["orig_cps"][0] == g["cp_count"]
+    if with_oracle:
+        cp = ora.sort_cp(ora.find_cp(d, eb), d)
+        s_ora = ora.encode_topo(d, eb, B, ora.mark_types(cp, dims))
+        sp = ora.extract_sp(cp)
+        assert topo_b == s_ora
+        assert sort_b == (ora.encode_ints(sp, B) if len(sp) else b"")
+        oraw, ofn, _ = ora.decode_topo(s_ora, d.size, eb, B)
+        assert (raw_h.view(np.int32) == oraw.view(np.int32)).all()
+        opost, _ = ora.post(oraw.reshape(dims), oraw.reshape(dims), ofn.reshape(dims), sp, eb)
+        assert (post_h.view(np.int32) == opost.reshape(-1).view(np.int32)).all()
+        orep = ora.topo_report(d, post_h.reshape(dims), eb)
+        for k, v in orep.items():
+            assert rep[k] == (pytest.approx(v) if k == "max_err" else v), k
+    ctx.close()
+    del dd, topo, sort, idx, raw, post, tys
+    torch.cuda.empty_cache()
+    # the reference entry points: critical points found and ranked on the GPU
+    cp = T.find_critical_points(d, eb)
+    scp = T.sort_critical_points(cp, d)
+    assert digest(scp.tobytes()) == g["cp"]
+    return rep
+
+
+def test_c1_2d_1800x3600(T, ora):
+    _single(T, ora, synth.config1(), gold()["c1"], with_oracle=True)
+
+
+def test_c2_3d_100x500x500_rel(T, ora):
+    _single(T, ora, synth.config2(), gold()["c2"], with_oracle=True)
+
+
+def test_c3_3d_512(T, ora):
+    _single(T, ora, synth.config3(), gold()["c3"], with_oracle=False)
+
+
+def test_c4_batch_256_fields(T):
+    import torch
+    g = gold()["c4"]
+    specs = synth.batch_specs(256, 3)
+    items = []
+    for k, sp in enumerate(specs):
+        f = synth.batch_field(sp, k)
+        assert digest(f.data.tobytes()) == g[k]["field"]
+        items.append((torch.from_numpy(f.data.reshape(-1)).cuda(), f.dims, float(sp[2]), sp[1] == "rel"))
+    b = T.Batch(64)
+    res = b.compress(items)
+    for k, (r, gk) in enumerate(zip(res, g)):
+        topo, sort, sizes, abs_eb = r
+        assert np.float32(abs_eb) == np.float32(gk["abs_eb"]), k
+        assert (sizes.cp_count, sizes.extrema_count) == (gk["cp_count"], gk["extrema"]), k
+        assert digest(topo[: sizes.topo_bytes].cpu().numpy().tobytes()) == gk["topo"], k
+        assert digest(sort[: sizes.sort_bytes].cpu().numpy().tobytes()) == gk["sort"], k
+    b.close()

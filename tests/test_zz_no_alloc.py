@@ -62,16 +62,62 @@ def test_noalloc_matches_workspace_encoder(T, case):
     assert _noalloc_stream(T, a, dims, eb, B) == ref_a
 
 
+def _raw_call(T, d, dims, eb, B, out, cap):
+    n = C.c_size_t(0)
+    rc = T.lib().szp_b200_topo_encode_noalloc(C.c_void_p(d.data_ptr()), T.geom_of(dims), eb, B,
+                                              C.c_void_p(out.data_ptr()), cap, C.byref(n), None)
+    return rc, n.value
+
+
 def test_noalloc_rejects_fields_beyond_the_scratch(T):
     """A field needing more tile descriptors than the fixed scratch holds is
-    rejected on the host before anything is launched or read."""
+    rejected on the host before anything is launched or read (the C ABI is
+    called directly with a small buffer: nothing may touch it)."""
     import torch
     tiny = torch.zeros(16, dtype=torch.float32, device="cuda")
     out = torch.zeros(64, dtype=torch.uint8, device="cuda")
-    with pytest.raises(T.ToposzpError, match="fixed scratch"):
-        T.encode_noalloc(tiny, (1024, 1024, 512), 1e-3, 64, out)
-    with pytest.raises(T.ToposzpError, match="blockSize"):
-        T.encode_noalloc(tiny, (4, 4), 1e-3, 300, out)
+    # 2^28 + 2048 elements: one tile of 2048 beyond the limit at blockSize 64
+    rc, _ = _raw_call(T, tiny, (131073, 2048), 1e-3, 64, out, 64)
+    assert rc == -1 and "fixed scratch" in T.last_error()
+    rc, _ = _raw_call(T, tiny, (1024, 1024, 1024), 1e-3, 64, out, 64)
+    assert rc == -1 and "fixed scratch" in T.last_error()
+    rc, _ = _raw_call(T, tiny, (4, 4), 1e-3, 300, out, 64)
+    assert rc == -1 and "blockSize" in T.last_error()
+    # extents whose product overflows are invalid geometry, not a small field
+    rc, _ = _raw_call(T, tiny, (2**31 - 1, 2**31 - 1, 2**31 - 1), 1e-3, 64, out, 64)
+    assert rc == -1 and "geometry" in T.last_error()
+    assert (out.cpu().numpy() == 0).all()
+
+
+def test_noalloc_accepts_the_largest_field(T):
+    """Exactly 2^28 elements at blockSize 64 fill the fixed scratch and are
+    accepted (a constant field: no critical points, 21-byte blocks)."""
+    import torch
+    dims = (512, 512, 1024)
+    d = torch.zeros(int(np.prod(dims)), dtype=torch.float32, device="cuda")
+    nblk = d.numel() // 64
+    cap = 8 + 21 * nblk + 64
+    out = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    nbytes = T.encode_noalloc(d, dims, 1e-3, 64, out)
+    assert nbytes == 8 + 21 * nblk
+    head = out[:8 + 21 * 2].cpu().numpy()
+    assert (head[:8] == 0).all()
+    # block: anchor 0, bit count 0, 16 tag bytes 0
+    assert (head[8:] == 0).all()
+    del d, out
+    torch.cuda.empty_cache()
+
+
+def test_noalloc_wrapper_checks_tensors(T):
+    import torch
+    d = torch.zeros(16, dtype=torch.float32, device="cuda")
+    out = torch.zeros(4096, dtype=torch.uint8, device="cuda")
+    with pytest.raises(T.ToposzpError, match="elements"):
+        T.encode_noalloc(d, (1024, 1024, 512), 1e-3, 64, out)
+    with pytest.raises(T.ToposzpError, match="float32"):
+        T.encode_noalloc(d.double(), (4, 4), 1e-3, 64, out)
+    with pytest.raises(T.ToposzpError, match="uint8"):
+        T.encode_noalloc(d, (4, 4), 1e-3, 64, out.int())
 
 
 def test_noalloc_output_too_small_is_an_error(T):

@@ -42,6 +42,21 @@ Geom make_geom(int nd, long long a, long long b, long long c) {
   return g;
 }
 
+bool geom_elements(const szp_b200_geom &g, unsigned long long *n, Geom *out) {
+  unsigned long long p = 1;
+  if (g.nd != 2 && g.nd != 3) return false;
+  for (int i = 0; i < g.nd; i++) {
+    if (g.dims[i] <= 0) return false;
+    if (__builtin_mul_overflow(p, (unsigned long long)g.dims[i], &p)) return false;
+  }
+  // the product of the extents must not wrap, and flat indices +- one plane
+  // stay far inside 64 bits
+  if (p >= kMaxElements) return false;
+  *out = (g.nd == 2) ? make_geom(2, g.dims[0], g.dims[1], 1) : make_geom(3, g.dims[0], g.dims[1], g.dims[2]);
+  *n = p;
+  return true;
+}
+
 static bool check_block_size(int B, const char *fn) {
   if (B <= 0 || B > kMaxBlockSize) {
     set_error("%s: blockSize %d out of range [1, %d]", fn, B, kMaxBlockSize);
@@ -638,17 +653,7 @@ size_t szp_b200_sort_bound(size_t n, int blockSize) {
 namespace tsz {
 
 static bool geom_ok(const szp_b200_geom &g, unsigned long long *n, Geom *out) {
-  if (g.nd == 2) {
-    if (g.dims[0] <= 0 || g.dims[1] <= 0) return false;
-    *out = make_geom(2, g.dims[0], g.dims[1], 1);
-  } else if (g.nd == 3) {
-    if (g.dims[0] <= 0 || g.dims[1] <= 0 || g.dims[2] <= 0) return false;
-    *out = make_geom(3, g.dims[0], g.dims[1], g.dims[2]);
-  } else {
-    return false;
-  }
-  *n = (unsigned long long)(out->d1 * out->d2 * out->d3);
-  return true;
+  return geom_elements(g, n, out);
 }
 
 }  // namespace tsz

@@ -756,12 +756,8 @@ int szp_b200_batch_compress(szp_b200_batch *b, szp_b200_batch_field *fs, int cou
     Geom g;
     const szp_b200_geom &gg = fs[f].geom;
     if (!fs[f].d_data || !fs[f].d_topo || !fs[f].d_sort) { set_error("field %d: null pointer", f); return -1; }
-    if (gg.nd == 2 && gg.dims[0] > 0 && gg.dims[1] > 0) g = make_geom(2, gg.dims[0], gg.dims[1], 1);
-    else if (gg.nd == 3 && gg.dims[0] > 0 && gg.dims[1] > 0 && gg.dims[2] > 0)
-      g = make_geom(3, gg.dims[0], gg.dims[1], gg.dims[2]);
-    else { set_error("field %d: invalid geometry", f); return -1; }
+    if (!geom_elements(gg, &n, &g)) { set_error("field %d: invalid geometry", f); return -1; }
     if (!(fs[f].errBound > 0.0f)) { set_error("field %d: error bound must be positive", f); return -1; }
-    n = (unsigned long long)(g.d1 * g.d2 * g.d3);
     if (fs[f].topo_cap < 8 || fs[f].sort_cap < 8) { set_error("field %d: output buffer too small", f); return -1; }
     plan[f].n = n;
     plan[f].nb = (n + B - 1) / B;

@@ -86,23 +86,18 @@ extern "C" SZP_B200_API int szp_b200_topo_encode_noalloc(const float *d_data, sz
     return -1;
   }
   Geom g;
-  if (geom.nd == 2 && geom.dims[0] > 0 && geom.dims[1] > 0) {
-    g = make_geom(2, geom.dims[0], geom.dims[1], 1);
-  } else if (geom.nd == 3 && geom.dims[0] > 0 && geom.dims[1] > 0 && geom.dims[2] > 0) {
-    g = make_geom(3, geom.dims[0], geom.dims[1], geom.dims[2]);
-  } else {
+  unsigned long long n = 0;
+  if (!geom_elements(geom, &n, &g)) {
     set_error("szp_b200_topo_encode_noalloc: invalid geometry");
     return -1;
   }
-  const unsigned long long n = (unsigned long long)(g.d1 * g.d2 * g.d3);
   const unsigned long long nb = (n + blockSize - 1) / blockSize;
   const unsigned long long tb = (unsigned long long)enc_tile_blocks(blockSize);
   const unsigned long long ntiles = (nb + tb - 1) / tb;
-  if (ntiles + 1 > kNoAllocTiles) {
+  if (ntiles > kNoAllocTiles) {
     set_error("szp_b200_topo_encode_noalloc: %llu elements need %llu tile descriptors, the fixed "
               "scratch holds %zu (at most %llu elements at blockSize %d)",
-              n, ntiles + 1, kNoAllocTiles, (unsigned long long)(kNoAllocTiles - 1) * tb * blockSize,
-              blockSize);
+              n, ntiles, kNoAllocTiles, (unsigned long long)kNoAllocTiles * tb * blockSize, blockSize);
     return -1;
   }
   if (topo_cap < 8) {
@@ -119,7 +114,7 @@ extern "C" SZP_B200_API int szp_b200_topo_encode_noalloc(const float *d_data, sz
   unsigned long long *w = reinterpret_cast<unsigned long long *>(base + kNoAllocTiles * sizeof(TileDesc));
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
   // scratch keeps the previous call's contents: clear what the kernel expects at zero
-  if (cuda_fail(cudaMemsetAsync(desc, 0, (ntiles + 1) * sizeof(TileDesc), s), "memset") ||
+  if (cuda_fail(cudaMemsetAsync(desc, 0, ntiles * sizeof(TileDesc), s), "memset") ||
       cuda_fail(cudaMemsetAsync(w, 0, kNoAllocWords * 8, s), "memset") ||
       cuda_fail(cudaMemsetAsync(d_topo, 0, 8, s), "memset"))
     return -1;

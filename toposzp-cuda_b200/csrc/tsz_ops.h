@@ -8,6 +8,14 @@ namespace tsz {
 // Geometry from extents (nd = 2: rows, cols; nd = 3: d1, d2, d3).
 Geom make_geom(int nd, long long a, long long b, long long c);
 
+// Largest element count a field may have (2^40): larger products, and
+// products of the extents that overflow, are rejected as invalid geometry.
+constexpr unsigned long long kMaxElements = 1ull << 40;
+
+// Validates a C-ABI geometry (nd 2 or 3, positive extents, element count
+// below kMaxElements without overflow) and fills the kernel geometry.
+bool geom_elements(const szp_b200_geom &g, unsigned long long *n, Geom *out);
+
 // Runs one encoder pass on ctx->stream and waits for it.
 //   out: payload destination (stream base + 8); the 8-byte header is written here too.
 //   totals_out (host): payload bytes, cps, extrema.

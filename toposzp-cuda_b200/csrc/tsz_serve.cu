@@ -23,6 +23,7 @@
 #include <thread>
 #include <vector>
 
+#include "tsz_ops.h"
 #include "tsz_runtime.h"
 
 namespace {
@@ -40,12 +41,11 @@ struct Slot {
   cudaStream_t stream = nullptr;
 };
 
+// element count of a request's geometry (0 when invalid or overflowing)
 size_t elems_of(const szp_b200_geom &g) {
-  if (g.nd == 2) return (size_t)(g.dims[0] > 0 ? g.dims[0] : 0) * (size_t)(g.dims[1] > 0 ? g.dims[1] : 0);
-  if (g.nd == 3)
-    return (size_t)(g.dims[0] > 0 ? g.dims[0] : 0) * (size_t)(g.dims[1] > 0 ? g.dims[1] : 0) *
-           (size_t)(g.dims[2] > 0 ? g.dims[2] : 0);
-  return 0;
+  unsigned long long n = 0;
+  tsz::Geom kg;
+  return tsz::geom_elements(g, &n, &kg) ? (size_t)n : 0;
 }
 
 }  // namespace

@@ -49,6 +49,7 @@ EXPORTS = [
     "szp_b200_topo_compress_host",
     "szp_b200_topo_decompress_host",
     "szp_b200_topo_encode_noalloc",
+    "szp_b200_topo_check",
     "szp_b200_batch_create",
     "szp_b200_batch_destroy",
     "szp_b200_batch_configure",
@@ -102,6 +103,20 @@ class ServerStats(C.Structure):
                 ("max_inflight_bytes", C.c_size_t), ("max_concurrent", C.c_int)]
 
 
+class TopoReport(C.Structure):
+    _fields_ = [("orig_cps", C.c_uint64 * 4), ("dec_cps", C.c_uint64 * 4), ("preserved", C.c_uint64),
+                ("lost", C.c_uint64), ("changed", C.c_uint64), ("new_cps", C.c_uint64),
+                ("lost_by_type", C.c_uint64 * 4), ("pairs", C.c_uint64 * 4), ("violations", C.c_uint64 * 4),
+                ("over_1eb", C.c_uint64), ("over_2eb", C.c_uint64), ("max_err", C.c_double)]
+
+    def as_dict(self) -> dict:
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            d[name] = list(v) if hasattr(v, "__len__") else v
+        return d
+
+
 class BatchField(C.Structure):
     _fields_ = [("d_data", C.c_void_p), ("geom", Geom), ("errBound", C.c_float), ("rel", C.c_int),
                 ("d_topo", C.c_void_p), ("topo_cap", C.c_size_t), ("d_sort", C.c_void_p),
@@ -153,6 +168,7 @@ def lib():
             "szp_b200_topo_compress_host": (i, [vp, vp, Geom, f, i, vp, sz, vp, sz, C.POINTER(Sizes)]),
             "szp_b200_topo_decompress_host": (i, [vp, vp, sz, vp, sz, Geom, f, i, vp, i]),
             "szp_b200_topo_encode_noalloc": (i, [vp, Geom, f, i, vp, sz, C.POINTER(sz), vp]),
+            "szp_b200_topo_check": (i, [vp, vp, vp, Geom, f, C.POINTER(TopoReport)]),
             "szp_b200_batch_create": (vp, [vp, i]),
             "szp_b200_batch_destroy": (None, [vp]),
             "szp_b200_batch_configure": (i, [vp, i, i]),
@@ -304,6 +320,17 @@ def encode_noalloc(d_data, shape, eb: float, block_size: int, d_topo, stream_han
     """Topology stream of a device field into the caller's uint8 device
     tensor d_topo, with no allocation inside the library; returns the stream
     length in bytes.  Calls on one device must not overlap."""
+    import torch
+    n = int(np.prod(shape))
+    if not (d_data.is_cuda and d_data.dtype == torch.float32 and d_data.is_contiguous()):
+        raise ToposzpError("encode_noalloc: d_data must be a contiguous float32 CUDA tensor")
+    if d_data.numel() != n:
+        raise ToposzpError("encode_noalloc: d_data holds %d elements, the shape %s needs %d"
+                           % (d_data.numel(), tuple(shape), n))
+    if not (d_topo.is_cuda and d_topo.dtype == torch.uint8 and d_topo.is_contiguous()):
+        raise ToposzpError("encode_noalloc: d_topo must be a contiguous uint8 CUDA tensor")
+    if d_topo.device != d_data.device:
+        raise ToposzpError("encode_noalloc: d_data and d_topo are on different devices")
     nbytes = C.c_size_t(0)
     rc = lib().szp_b200_topo_encode_noalloc(
         C.c_void_p(d_data.data_ptr()), geom_of(shape), eb, block_size, C.c_void_p(d_topo.data_ptr()),
@@ -400,6 +427,15 @@ class Context:
         if rc:
             raise ToposzpError(last_error())
         return h_out
+
+    def topo_check(self, d_orig, d_dec, shape, eb: float) -> dict:
+        """Topology report of a decompressed device field against the original."""
+        rep = TopoReport()
+        rc = lib().szp_b200_topo_check(self.ptr, C.c_void_p(d_orig.data_ptr()), C.c_void_p(d_dec.data_ptr()),
+                                       geom_of(shape), eb, C.byref(rep))
+        if rc:
+            raise ToposzpError(last_error())
+        return rep.as_dict()
 
     def postprocess(self, d_data, d_orig, d_types_int, d_sp, shape, eb: float, axis_stencil=False):
         rc = lib().szp_b200_topo_postprocess_dev(
