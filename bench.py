@@ -414,6 +414,7 @@ def serve_leg(T, dev, nreq=400, slots=4, rate=2000.0, seed=4):
     sizes = T.Sizes()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     svc = np.zeros(nreq)
+    stage_rows = [None] * nreq
     for rep in range(2):
         for i, sp in enumerate(spec):
             dims = pool[sp[1]][0]
@@ -432,6 +433,28 @@ def serve_leg(T, dev, nreq=400, slots=4, rate=2000.0, seed=4):
             ev[1].record(stream)
             ev[1].synchronize()
             svc[i] = ev[0].elapsed_time(ev[1]) * 1e-3
+            stage_rows[i] = ctx.stage_times()
+    # where the plain calls spend their device time: per op and size decile,
+    # the summed stage times (CUDA events on the workspace stream)
+    sizes_b = np.array([4.0 * np.prod(pool[sp[1]][0]) for sp in spec])
+    edges = np.quantile(sizes_b, np.linspace(0, 1, 11))
+    breakdown = []
+    for op in ("c", "d"):
+        for k in range(10):
+            sel = [i for i, sp in enumerate(spec) if sp[0] == op and
+                   edges[k] <= sizes_b[i] <= edges[k + 1] and (k == 9 or sizes_b[i] < edges[k + 1])]
+            if not sel:
+                continue
+            st = {}
+            for i in sel:
+                for name, ms in stage_rows[i]:
+                    st[name] = st.get(name, 0.0) + ms
+            mb = float(sizes_b[sel].sum() / 1e6)
+            tsum = float(svc[sel].sum())
+            breakdown.append({"op": "compress" if op == "c" else "decompress", "decile": k,
+                              "requests": len(sel), "mb": round(mb, 1), "device_s": round(tsum, 4),
+                              "gbs": round(mb / 1e3 / tsum, 2) if tsum > 0 else None,
+                              "stages_ms": {kk: round(v, 2) for kk, v in sorted(st.items(), key=lambda x: -x[1])}})
     t = 0.0
     plat = np.zeros(nreq)
     for i in range(nreq):
@@ -448,7 +471,8 @@ def serve_leg(T, dev, nreq=400, slots=4, rate=2000.0, seed=4):
            "plain_busy_s": float(svc.sum()), "served_span_s": float(span),
            "batches": st["batches"] - st0["batches"],
            "batched_requests": st["batched_requests"] - st0["batched_requests"],
-           "max_concurrent": st["max_concurrent"], "max_inflight_gb": st["max_inflight_bytes"] / 1e9}
+           "max_concurrent": st["max_concurrent"], "max_inflight_gb": st["max_inflight_bytes"] / 1e9,
+           "plain_breakdown": breakdown}
     srv.close()
     ctx.close()
     return out
