@@ -232,6 +232,17 @@ SZP_B200_API int szp_b200_topo_check(szp_b200_ctx *ctx, const float *d_orig, con
                                      szp_b200_geom geom, float absErrBound,
                                      szp_b200_topo_report *report);
 
+/* Bounded-wait self-test (no reference counterpart).  Every device wait of
+ * the library gives up after a poll limit and reports an error instead of
+ * hanging; this runs one such wait that can never be satisfied, with a short
+ * limit (spin_limit polls, 1 .. 2^20), and returns the status it ended with:
+ *   which = 0: a tile look-back whose predecessor never publishes
+ *              (expected status 1, look-back timeout);
+ *   which = 1: a grid barrier that one CTA never reaches
+ *              (expected status 5, wait timeout).
+ * *ms is the probe kernel's device time.  Returns 0 when the probe ran. */
+SZP_B200_API int szp_b200_selftest_bounded_wait(int which, int spin_limit, int *status, float *ms);
+
 /* ------------------------------------------------------------------ */
 /* Batched compression (no reference counterpart)                      */
 /* ------------------------------------------------------------------ */

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "tsz_enc64.h"
 #include "tsz_ops.h"
 
 namespace tsz {
@@ -107,7 +108,9 @@ int encode_pass(szp_b200_ctx *ctx, int mode, const float *d_data, const int *d_i
   a.cp_cap = cp_cap;
   int grid = (int)std::min<unsigned long long>(ntiles, (unsigned long long)ctx->sm_count * 8ull);
   if (grid < 1) grid = 1;
-  if (cuda_fail(launch_encode(mode, a, s, grid), "encode launch")) return -1;
+  if (cuda_fail(enc64_applies(a, mode) ? launch_enc64_from(a, s, ctx->sm_count) : launch_encode(mode, a, s, grid),
+                "encode launch"))
+    return -1;
   ctx->launches += 1;
   if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 8 * sizeof(unsigned long long),
                                 cudaMemcpyDeviceToHost, s), "D2H totals") ||
@@ -191,7 +194,10 @@ static int encode_topo_chunked(szp_b200_ctx *ctx, const float *h_src, float *d_d
     a.tile_hi = upto;
     if (cuda_fail(cudaMemsetAsync(w + 3, 0, 8, s), "memset")) return -1;
     const int grid = (int)std::min<unsigned long long>(upto - done, (unsigned long long)ctx->sm_count * 8ull);
-    if (cuda_fail(launch_encode(kEncClassify, a, s, grid), "encode launch")) return -1;
+    if (cuda_fail(enc64_applies(a, kEncClassify) ? launch_enc64_from(a, s, ctx->sm_count)
+                                                 : launch_encode(kEncClassify, a, s, grid),
+                  "encode launch"))
+      return -1;
     ctx->launches += 1;
     done = upto;
     if (h_out && upto < ntiles) {

@@ -107,9 +107,11 @@ namespace tsz {
 // tile's aggregate has been published.  Each round inspects one predecessor
 // per thread, so a walk back over P in-flight tiles takes about P / (WARPS *
 // 32) rounds instead of P / 32.
+// spin_limit: polls of one predecessor before the wait gives up (0: kSpinLimit)
 template <int WARPS = kWarps>
 __device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long long agg_bytes,
-                                      unsigned long long agg_cnt, int *err) {
+                                      unsigned long long agg_cnt, int *err, int spin_limit = 0) {
+  const int limit = spin_limit > 0 ? spin_limit : kSpinLimit;
   __shared__ unsigned s_first[WARPS];
   __shared__ unsigned long long s_b[WARPS], s_c[WARPS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -124,7 +126,7 @@ __device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long
       st = ld_acquire_u64(&desc[idx].status);
       int spins = 0;
       while ((st >> kStatShift) == 0ull) {
-        if (++spins > kSpinLimit) { timed_out = true; break; }
+        if (++spins > limit) { timed_out = true; break; }
         __nanosleep(spins < 64 ? 32 : 256);
         st = ld_acquire_u64(&desc[idx].status);
       }

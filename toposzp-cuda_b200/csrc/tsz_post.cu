@@ -83,6 +83,7 @@ struct PostArgs {
   const unsigned *XP;           // per bitmap word: list position of its first extremum (X entries before it)
   int *err;
   unsigned *restored;
+  int spin_limit;               // grid-barrier polls before giving up (0: default)
 };
 
 __device__ __forceinline__ unsigned long long ld_rlx(const unsigned long long *p) {
@@ -817,7 +818,8 @@ __device__ __forceinline__ void st_rel_u32(unsigned *p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, int spin_limit = 0) {
+  const int limit = spin_limit > 0 ? spin_limit : kBarSpinLimit;
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -834,7 +836,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
       int spins = 0;
       unsigned nap = 64;
       while (ld_acq_u32(bar + 1) == g) {
-        if (++spins > kBarSpinLimit) {
+        if (++spins > limit) {
           ok = 0;
           atomicExch(err, kErrWaitTimeout);
           break;
@@ -895,7 +897,7 @@ pass_coop_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *
       wb = __shfl_sync(0xffffffffu, wb, 0);
       if (defer) Wn[wb + __popc(m & ((1u << lane) - 1u))] = idx;
     }
-    if (!grid_barrier(bar, a.err)) return;
+    if (!grid_barrier(bar, a.err, a.spin_limit)) return;
     const unsigned next = __ldcg(cnt);
     if ((round > 0 || after_round0) && next >= nw) {
       if (blockIdx.x == 0 && threadIdx.x == 0) status[0] = 2;
@@ -1261,6 +1263,38 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   if (ctx->h_words[9] == 2) { set_error("post-processing pass made no progress"); return -1; }
   if (restored_out) *restored_out = (int)(ctx->h_words[5] & 0xffffffffu);
   return 0;
+}
+
+// Bounded-wait check of the grid barrier: the last CTA of the launch leaves
+// without arriving, so the others must give up after spin_limit polls and
+// report kErrWaitTimeout (no CTA waits on anything that can hang).
+__global__ void barrier_timeout_probe_kernel(unsigned *bar, int *err, int spin_limit) {
+  if (blockIdx.x == gridDim.x - 1) return;
+  grid_barrier(bar, err, spin_limit);
+}
+
+int selftest_grid_barrier(int spin_limit, int *status, float *ms) {
+  unsigned *d = nullptr;
+  if (cuda_fail(cudaMalloc(&d, 64), "cudaMalloc")) return -1;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = -1;
+  if (!cuda_fail(cudaMemset(d, 0, 64), "memset") && !cuda_fail(cudaEventCreate(&e0), "event") &&
+      !cuda_fail(cudaEventCreate(&e1), "event")) {
+    cudaEventRecord(e0, 0);
+    barrier_timeout_probe_kernel<<<2, 64>>>(d, reinterpret_cast<int *>(d + 4), spin_limit);
+    cudaEventRecord(e1, 0);
+    int h = 0;
+    if (!cuda_fail(cudaGetLastError(), "probe launch") &&
+        !cuda_fail(cudaMemcpy(&h, d + 4, 4, cudaMemcpyDeviceToHost), "D2H")) {
+      cudaEventElapsedTime(ms, e0, e1);
+      *status = h;
+      rc = 0;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(d);
+  return rc;
 }
 
 int postprocess(szp_b200_ctx *ctx, float *d_data, const float *d_orig,

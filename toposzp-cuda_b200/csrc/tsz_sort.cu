@@ -18,6 +18,7 @@
 
 #include "tsz_ops.h"
 #include "tsz_lookback.cuh"
+#include "tsz_scan.cuh"
 
 namespace tsz {
 
@@ -468,7 +469,7 @@ __global__ void fb_gather_count_kernel(const unsigned *__restrict__ fb_list, uns
 __global__ void fb_gather_kernel(const unsigned *__restrict__ fb_list, unsigned nfb,
                                  const unsigned long long *__restrict__ start,
                                  const unsigned long long *__restrict__ fb_off,
-                                 const uint2 *__restrict__ recs, BinSrc bin_of,
+                                 const uint2 *__restrict__ recs, BinSrc bin_of, bool code_keys,
                                  unsigned long long *__restrict__ key,
                                  unsigned *__restrict__ val) {
   for (unsigned f = blockIdx.x; f < nfb; f += gridDim.x) {
@@ -476,7 +477,8 @@ __global__ void fb_gather_kernel(const unsigned *__restrict__ fb_list, unsigned 
     const unsigned long long o = fb_off[f];
     for (unsigned long long i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
       const uint2 r = recs[i];
-      key[o + (i - r0)] = ((unsigned long long)((unsigned)bin_of(r, i) ^ 0x80000000u) << 32) | r.x;
+      key[o + (i - r0)] = code_keys ? (unsigned long long)r.x
+                                    : (((unsigned long long)((unsigned)bin_of(r, i) ^ 0x80000000u) << 32) | r.x);
       val[o + (i - r0)] = r.y;
     }
   }
@@ -496,26 +498,6 @@ __global__ void radix_hist_kernel(const unsigned long long *__restrict__ key, un
   }
   __syncthreads();
   H[(size_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];  // digit-major
-}
-
-// exclusive scan of a u32 array in place (single CTA, used for small matrices)
-__global__ void scan_inplace_kernel(unsigned *__restrict__ a, unsigned long long n) {
-  __shared__ unsigned long long part[1024];
-  const unsigned long long per = (n + blockDim.x - 1) / blockDim.x;
-  const unsigned long long i0 = threadIdx.x * per;
-  unsigned long long s = 0;
-  for (unsigned long long i = 0; i < per; i++) if (i0 + i < n) s += a[i0 + i];
-  part[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-    unsigned long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
-  }
-  unsigned long long run = part[threadIdx.x] - s;
-  for (unsigned long long i = 0; i < per; i++)
-    if (i0 + i < n) { const unsigned v = a[i0 + i]; a[i0 + i] = (unsigned)run; run += v; }
 }
 
 // stable scatter: items of a tile are ranked in order, 256 at a time
@@ -557,51 +539,35 @@ __global__ void radix_scatter_kernel(const unsigned long long *__restrict__ key,
   }
 }
 
-// dense rank inside bins of the sorted fallback list (one CTA, sequential chunks)
-__global__ void fb_rank_kernel(const unsigned long long *__restrict__ key,
-                               const unsigned *__restrict__ val, unsigned long long n,
-                               int *__restrict__ out) {
-  __shared__ int carry_rank;
-  __shared__ int wsum[8];
-  __shared__ long long wlast_binstart[8];
-  if (threadIdx.x == 0) carry_rank = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (unsigned long long c = 0; c < n; c += blockDim.x) {
-    const unsigned long long i = c + threadIdx.x;
-    const bool in = i < n;
-    const unsigned long long k = in ? key[i] : 0ull;
-    const unsigned long long kp = (in && i > 0) ? key[i - 1] : k;
-    const bool newbin = in && (i == 0 || (k >> 32) != (kp >> 32));
-    const int inc = (in && i > 0 && !newbin && (unsigned)k != (unsigned)kp) ? 1 : 0;
-    // segmented inclusive scan of inc, segments start at newbin
-    int v = inc;
-    bool seg = newbin;
-    for (int o = 1; o < 32; o <<= 1) {
-      int tv = __shfl_up_sync(0xffffffffu, v, o);
-      bool ts = __shfl_up_sync(0xffffffffu, seg, o);
-      if (lane >= o && !seg) { v += tv; seg = ts; }
-    }
-    if (lane == 31) { wsum[warp] = v; wlast_binstart[warp] = seg ? 1 : 0; }
-    __syncthreads();
-    // combine warps sequentially (8 warps)
-    int pre = 0;
-    bool cut = false;
-    for (int w = warp - 1; w >= 0 && !cut; w--) {
-      pre += wsum[w];
-      if (wlast_binstart[w]) cut = true;
-    }
-    int rank;
-    if (seg) rank = v;                     // a bin started inside this warp before/at me
-    else if (cut) rank = v + pre;          // a bin started in an earlier warp of this chunk
-    else rank = v + pre + carry_rank;      // bin continues from the previous chunk
-    if (in && val[i] != kNoExtremum) out[val[i]] = rank;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1 || i == n - 1) {
-      if (in) carry_rank = rank;
-    }
-    __syncthreads();
-  }
+// Dense rank inside bins of the sorted fallback list, in parallel:
+//   A[i] = 1 where a new distinct key starts; D = inclusive sum of A
+//   H[i] = D[i] where a new bin starts (else 0); Dh = inclusive max of H
+//   rank[i] = D[i] - Dh[i]  (distinct keys of the bin before key i)
+// Keys are (bin, code) pairs, or codes alone when the bins follow from the
+// codes (a bin is a monotone function of the value).
+__device__ __forceinline__ unsigned long long fb_bin(unsigned long long k, bool code_keys, float eb, double inv) {
+  return code_keys ? (unsigned long long)(unsigned)quant_bin(code_float((unsigned)k), eb, inv) : (k >> 32);
+}
+
+__global__ void fb_distinct_kernel(const unsigned long long *__restrict__ key, unsigned long long n,
+                                   unsigned *__restrict__ A) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) A[i] = (i == 0 || key[i] != key[i - 1]) ? 1u : 0u;
+}
+
+__global__ void fb_heads_kernel(const unsigned long long *__restrict__ key, unsigned long long n,
+                                const unsigned *__restrict__ D, bool code_keys, float eb, double inv,
+                                unsigned *__restrict__ H) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bool head = i == 0 || fb_bin(key[i], code_keys, eb, inv) != fb_bin(key[i - 1], code_keys, eb, inv);
+  H[i] = head ? D[i] : 0u;
+}
+
+__global__ void fb_out_kernel(const unsigned *__restrict__ val, unsigned long long n, const unsigned *__restrict__ D,
+                              const unsigned *__restrict__ Dh, int *__restrict__ out) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && val[i] != kNoExtremum) out[val[i]] = (int)(D[i] - Dh[i]);
 }
 
 static int rank_fallback(szp_b200_ctx *ctx, const uint2 *recs, BinSrc bin_of, const unsigned long long *start,
@@ -675,7 +641,9 @@ int rank_positions(szp_b200_ctx *ctx, const uint2 *d_pairs, const int *d_bins,
 }
 
 // Buckets that did not fit the bitmap rank: their records are gathered and
-// ranked after a device-wide LSD radix sort on (bin, code).
+// ranked after a device-wide LSD radix sort on (bin, code) -- on the code
+// alone when the bins follow from the codes -- and a parallel segmented
+// distinct count.
 static int rank_fallback(szp_b200_ctx *ctx, const uint2 *recs, BinSrc bin_of, const unsigned long long *start,
                          const unsigned *fb_list, unsigned nfb, int *d_sp) {
   cudaStream_t s = ctx->stream;
@@ -695,21 +663,34 @@ static int rank_fallback(szp_b200_ctx *ctx, const uint2 *recs, BinSrc bin_of, co
   unsigned *v1 = A.take<unsigned>(nf), *v2 = A.take<unsigned>(nf);
   const unsigned ntiles = (unsigned)((nf + kRadixTile - 1) / kRadixTile);
   unsigned *H = A.take<unsigned>((size_t)256 * ntiles);
-  if (!fb_off || !k1 || !k2 || !v1 || !v2 || !H) {
+  const unsigned long long hn = (unsigned long long)256 * ntiles;
+  unsigned *part = A.take<unsigned>(scan_parts(hn > nf ? hn : nf));
+  if (!fb_off || !k1 || !k2 || !v1 || !v2 || !H || !part) {
     set_error("scratch arena too small for the rank fallback");
     return -1;
   }
+  const bool code_keys = bin_of.bins == nullptr;
   cudaMemcpyAsync(fb_off, h_off.data(), nfb * 8, cudaMemcpyHostToDevice, s);
-  fb_gather_kernel<<<std::min(nfb, 4096u), 256, 0, s>>>(fb_list, nfb, start, fb_off, recs, bin_of, k1, v1);
-  for (int shift = 0; shift < 64; shift += 8) {
+  fb_gather_kernel<<<std::min(nfb, 4096u), 256, 0, s>>>(fb_list, nfb, start, fb_off, recs, bin_of, code_keys, k1,
+                                                          v1);
+  const int bits = code_keys ? 32 : 64;
+  for (int shift = 0; shift < bits; shift += 8) {
     radix_hist_kernel<<<ntiles, 256, 0, s>>>(k1, nf, shift, H, ntiles);
-    scan_inplace_kernel<<<1, 1024, 0, s>>>(H, (unsigned long long)256 * ntiles);
+    if (cuda_fail(device_scan_u32<OpAdd>(H, H, hn, part, false, s), "scan")) return -1;
     radix_scatter_kernel<<<ntiles, 256, 0, s>>>(k1, v1, nf, shift, H, ntiles, k2, v2);
     std::swap(k1, k2);
     std::swap(v1, v2);
   }
-  fb_rank_kernel<<<1, 256, 0, s>>>(k1, v1, nf, d_sp);
-  ctx->launches += 3 + 8 * 3;
+  // k2 / v2 are free now: D in the key storage of k2, Dh beside it
+  unsigned *D = reinterpret_cast<unsigned *>(k2);
+  unsigned *Dh = D + nf;
+  const unsigned g = (unsigned)((nf + 255) / 256);
+  fb_distinct_kernel<<<g, 256, 0, s>>>(k1, nf, D);
+  if (cuda_fail(device_scan_u32<OpAdd>(D, D, nf, part, true, s), "scan")) return -1;
+  fb_heads_kernel<<<g, 256, 0, s>>>(k1, nf, D, code_keys, bin_of.eb, bin_of.inv, Dh);
+  if (cuda_fail(device_scan_u32<OpMax>(Dh, Dh, nf, part, true, s), "scan")) return -1;
+  fb_out_kernel<<<g, 256, 0, s>>>(v1, nf, D, Dh, d_sp);
+  ctx->launches += 3 + (bits / 8) * 5 + 9;
   if (cuda_fail(cudaGetLastError(), "fallback kernels") ||
       cuda_fail(cudaStreamSynchronize(s), "fallback"))
     return -1;
@@ -770,7 +751,8 @@ size_t rank_scratch_bytes_seg(unsigned long long K, int F, int sm_count) {
   const unsigned long long chunk = std::max<unsigned long long>(4096, (K + 2 * sm_count - 1) / (2 * sm_count));
   const size_t C = (size_t)(K / chunk) + (size_t)F + 1;
   const size_t nbk = (size_t)F * NB;
-  const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4);
+  const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4) +
+                    a256(scan_parts(256 * ((K + kRadixTile - 1) / kRadixTile) + K) * 4);
   return a256(C * sizeof(SegChunk)) + a256((F + 1) * 4) + a256(C * NB * 4) + a256(nbk * 4) +
          a256((nbk + 1) * 8) + a256(K * 8) + a256(K * 4) + a256(nbk * 4) * 2 + a256(16) + fb + a256(nbk * 8) + 8192;
 }
@@ -781,7 +763,8 @@ size_t rank_scratch_bytes(unsigned long long K, int sm_count) {
   const size_t NB = (size_t)1 << logNB;
   const size_t G = (size_t)sm_count * 2 + 1;
   // fallback worst case: all K records (two key/value ping-pong buffers + histogram)
-  const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4);
+  const size_t fb = a256(K * 8) * 2 + a256(K * 4) * 2 + a256(256 * ((K + kRadixTile - 1) / kRadixTile) * 4) +
+                    a256(scan_parts(256 * ((K + kRadixTile - 1) / kRadixTile) + K) * 4);
   // records (8 B) and, for given bins, their permuted bins (4 B)
   return a256(G * NB * 4) + a256(NB * 4) + a256((NB + 1) * 8) + a256(K * 8) + a256(K * 4) +
          a256(NB * 4) * 3 + a256(16) + fb + a256((NB + 1) * 8) * 2 + 4096;

@@ -50,6 +50,7 @@ EXPORTS = [
     "szp_b200_topo_decompress_host",
     "szp_b200_topo_encode_noalloc",
     "szp_b200_topo_check",
+    "szp_b200_selftest_bounded_wait",
     "szp_b200_batch_create",
     "szp_b200_batch_destroy",
     "szp_b200_batch_configure",
@@ -169,6 +170,7 @@ def lib():
             "szp_b200_topo_decompress_host": (i, [vp, vp, sz, vp, sz, Geom, f, i, vp, i]),
             "szp_b200_topo_encode_noalloc": (i, [vp, Geom, f, i, vp, sz, C.POINTER(sz), vp]),
             "szp_b200_topo_check": (i, [vp, vp, vp, Geom, f, C.POINTER(TopoReport)]),
+            "szp_b200_selftest_bounded_wait": (i, [i, i, C.POINTER(i), C.POINTER(f)]),
             "szp_b200_batch_create": (vp, [vp, i]),
             "szp_b200_batch_destroy": (None, [vp]),
             "szp_b200_batch_configure": (i, [vp, i, i]),
