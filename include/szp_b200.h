@@ -232,6 +232,42 @@ SZP_B200_API int szp_b200_topo_check(szp_b200_ctx *ctx, const float *d_orig, con
                                      szp_b200_geom geom, float absErrBound,
                                      szp_b200_topo_report *report);
 
+/* ------------------------------------------------------------------ */
+/* .SZp container and the OpenMP stream layouts                        */
+/* ------------------------------------------------------------------ */
+/* The container the reference's CPU drivers write and read
+ * (example/testfloat_compress_fastmode1_topology.cc:105-125,
+ * example/testfloat_decompress_fastmode1_topology.cc:720-805):
+ *   [topology stream][sort-position stream][u64 topology size][u64 sort size]
+ * with the streams in the reference's OpenMP layout
+ * (SZp/src/szp_float.cc:522-865, 999-1318; SZp/src/szp_topology_3d.cc:253-632):
+ *   topology       [u64 offset x T][blocks]
+ *   sort positions [u64 E][u64 offset x T][blocks]   (absent when E == 0)
+ * T = the writer's thread count; a one-element block carries its (zero)
+ * bit-count byte.  Device pointers; synchronous on the workspace stream. */
+
+/* Bytes a container of n elements may need with `threads` chunks. */
+SZP_B200_API size_t szp_b200_container_bound(size_t n, int blockSize, int threads);
+
+/* Container from the CUDA-layout streams of szp_b200_topo_compress_dev (the
+ * bytes the reference's CPU compressor writes with `threads` OpenMP threads,
+ * 1..128, for the same critical-point order).  extrema: sizes.extrema_count.
+ * blockSize <= 256.  Returns 0 on success. */
+SZP_B200_API int szp_b200_container_from_streams_dev(szp_b200_ctx *ctx, const unsigned char *d_topo,
+                                                     size_t topo_bytes, const unsigned char *d_sort,
+                                                     size_t sort_bytes, szp_b200_geom geom, int blockSize,
+                                                     size_t extrema, int threads, unsigned char *d_out,
+                                                     size_t out_cap, size_t *out_bytes);
+
+/* Decompression (+ post-processing, as szp_b200_topo_decompress_dev) of a
+ * container written by the reference's CPU path with any thread count, or
+ * by the call above.  The thread counts of both streams are detected by the
+ * reference's rule (SZp/include/szp_detect_threads.h:153-190, 282-309), every
+ * chunk walked by the device parser.  blockSize <= 256. */
+SZP_B200_API int szp_b200_container_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_in, size_t in_bytes,
+                                                   szp_b200_geom geom, float absErrBound, int blockSize,
+                                                   float *d_out, unsigned char *d_types, int postprocess);
+
 /* Bounded-wait self-test (no reference counterpart).  Every device wait of
  * the library gives up after a poll limit and reports an error instead of
  * hanging; this runs one such wait that can never be satisfied, with a short

@@ -25,5 +25,6 @@ def test_reference_arm_json_line():
     assert line["impl"] == "reference" and line["value"] > 0
     assert "workload" in line["config"]
     cb = line["cpu_baseline"]
-    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and "first 64 of 64 planes" in cb["sample"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and "the whole" in cb["sample"]
+    assert cb["one_thread"]["value"] > 0 and len(cb["slab_step_seconds"]) == 1 and cb["slab_value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0

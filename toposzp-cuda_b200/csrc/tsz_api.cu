@@ -759,11 +759,12 @@ namespace tsz {
 // d_blk_index == nullptr the block offsets of both streams are parsed on the
 // device; ref_bound selects the reference's validation bound for that parse
 // and *parse_failed reports a stream that is not a valid single-chunk stream.
-static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, size_t topo_bytes,
-                               const unsigned char *d_sort, size_t sort_bytes,
-                               const uint64_t *d_blk_index, szp_b200_geom geom, float absErrBound,
-                               int blockSize, float *d_out, unsigned char *d_types, int postprocess,
-                               bool ref_bound, bool *parse_failed, cudaEvent_t sort_ready = nullptr) {
+int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, size_t topo_bytes,
+                        const unsigned char *d_sort, size_t sort_bytes,
+                        const uint64_t *d_blk_index, szp_b200_geom geom, float absErrBound,
+                        int blockSize, float *d_out, unsigned char *d_types, int postprocess,
+                        bool ref_bound, bool *parse_failed, cudaEvent_t sort_ready, bool cpu_layout,
+                        unsigned long long sort_count) {
   if (parse_failed) *parse_failed = false;
   if (!ctx || !d_topo || !d_out) { set_error("null argument"); return -1; }
   if (!check_block_size(blockSize, "szp_b200_topo_decompress_dev")) return -1;
@@ -806,6 +807,8 @@ static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, s
   a.fn_u8 = T;
   a.err = reinterpret_cast<int *>(w + 4);
   a.ext_count = w + 6;
+  a.cpu_layout = cpu_layout ? 1 : 0;
+  if (cpu_layout && B > 256) { set_error("the OpenMP stream layout is read for blockSize <= 256"); return -1; }
   if (cuda_fail(launch_decode(true, a, s), "decode")) return -1;
   ctx->launches += 1;
   tl_mark(ctx, "decode_topo");
@@ -830,7 +833,8 @@ static int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, s
   }
   if (ctx->h_words[4] & 0xffffffffu) { set_error("decoder reported malformed stream"); return -1; }
   if (!post) return 0;
-  const unsigned long long E = ctx->h_words[6];
+  // sort positions: one per extremum tag, unless the caller knows the count
+  const unsigned long long E = sort_count != ~0ull ? sort_count : ctx->h_words[6];
   const int *spp = nullptr;
   if (E > 0 && have_sort) {
     if (parse && (ctx->h_words[18] == 0 || ctx->h_words[19] != 0)) {

@@ -45,7 +45,14 @@ struct DecArgs {
   int *err;
   unsigned long long *ext_count;  // optional: number of type-1/2 tags
   unsigned long long img_cap;   // set by the launcher
+  int cpu_layout;               // OpenMP layout: a one-element block carries its (zero) bit-count byte
 };
+
+// bytes of one block in the CUDA layout, or in the OpenMP layout (cpu), where
+// a one-element block also carries a bit-count byte
+__host__ __device__ __forceinline__ uint32_t block_bytes_layout(uint32_t n, uint32_t bc, bool tags, bool cpu) {
+  return (cpu && n == 1u) ? 5u + (tags ? 1u : 0u) : block_bytes(n, bc, tags);
+}
 
 int enc_tile_blocks(int B);   // codec blocks per encoder tile (look-back granularity)
 int octet_group(int B);       // lanes per codec block in the octet kernels (B <= 256)

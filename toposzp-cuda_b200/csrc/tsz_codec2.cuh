@@ -751,7 +751,7 @@ decode2_kernel(DecArgs a) {
     anchor = (int)((unsigned)img[start] | ((unsigned)img[start + 1] << 8) | ((unsigned)img[start + 2] << 16) |
                    ((unsigned)img[start + 3] << 24));
     if (len > 1) bc = (start + 4 < bend) ? img[start + 4] : 0u;
-    if (bc > 32u || start + block_bytes((unsigned)len, bc, TAGS) > bend) ok = false;
+    if (bc > 32u || start + block_bytes_layout((unsigned)len, bc, TAGS, a.cpu_layout != 0) > bend) ok = false;
   }
   if (have && !ok && l == 0) atomicExch(a.err, kErrMalformed);
   // deltas e0 .. e0+7
@@ -829,7 +829,8 @@ decode2_kernel(DecArgs a) {
       }
     }
     if (TAGS) {
-      const unsigned tsec = start + block_bytes((unsigned)len, bc, true) - ((unsigned)len + 3u) / 4u;
+      const unsigned tsec =
+          start + block_bytes_layout((unsigned)len, bc, true, a.cpu_layout != 0) - ((unsigned)len + 3u) / 4u;
       const unsigned tb = ((unsigned)len + 3u) / 4u;
       const unsigned b0t = (2u * l < tb) ? img[tsec + 2 * l] : 0u;
       const unsigned b1t = (2u * l + 1u < tb) ? img[tsec + 2 * l + 1] : 0u;

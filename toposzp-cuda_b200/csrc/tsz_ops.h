@@ -63,8 +63,22 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
 // payload offsets to d_offs and d_status[0] = payload length + 1 on success
 // (0 when the walk failed), d_status[1] = nonzero on a malformed block.
 size_t parse_scratch_bytes(unsigned long long buf_len, int B, bool tags);
+// cpu: the OpenMP layout, whose one-element blocks carry a bit-count byte.
 int parse_stream(szp_b200_ctx *ctx, Arena &A, const unsigned char *d_payload, unsigned long long buf_len,
                  unsigned long long n, const unsigned long long *d_n, int B, bool tags, bool ref_bound,
-                 unsigned long long *d_offs, unsigned long long *d_status);
+                 unsigned long long *d_offs, unsigned long long *d_status, bool cpu = false);
+
+// Fused decompression (+ post-processing) of device streams; d_topo / d_sort
+// point 8 bytes before their payloads.  With d_blk_index null the block
+// offsets are parsed on the device (single-chunk streams).  cpu_layout: the
+// topology stream's one-element blocks carry a bit-count byte (OpenMP layout).
+// sort_count: entries of the sort-position stream when the caller knows it
+// (a container header), else one per extremum tag.
+int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, size_t topo_bytes,
+                        const unsigned char *d_sort, size_t sort_bytes,
+                        const uint64_t *d_blk_index, szp_b200_geom geom, float absErrBound,
+                        int blockSize, float *d_out, unsigned char *d_types, int postprocess,
+                        bool ref_bound, bool *parse_failed, cudaEvent_t sort_ready = nullptr,
+                        bool cpu_layout = false, unsigned long long sort_count = ~0ull);
 
 }  // namespace tsz

@@ -45,11 +45,12 @@ struct ParseGeom {
   bool tags;
   unsigned full_tag;           // tag bytes of a full block
   unsigned M;                  // largest valid block (bit count 32)
+  bool cpu;                    // OpenMP layout: one-element blocks carry a bit-count byte
 };
 
 // length of a full block (B elements) from its bit count; 0 = invalid
 __device__ __forceinline__ unsigned full_block_len(const ParseGeom &g, unsigned bc) {
-  if (g.B == 1) return 4u + g.full_tag;
+  if (g.B == 1) return 4u + (g.cpu ? 1u : 0u) + g.full_tag;
   if (bc > 32u) return 0u;
   unsigned s = 5u + g.full_tag;
   if (bc) s += (unsigned)((g.B - 2) >> 3) + 1u + mag_bytes((unsigned)g.B - 1u, bc);
@@ -70,7 +71,7 @@ __global__ void __launch_bounds__(256) parse_seg_kernel(ParseGeom g, unsigned lo
       c++;
       unsigned len;
       if (g.B == 1) {
-        len = 4u + g.full_tag;
+        len = 4u + (g.cpu ? 1u : 0u) + g.full_tag;
       } else {
         if (p + 4 >= g.len) break;   // bit count byte outside the buffer
         len = full_block_len(g, __ldg(g.p + p + 4));
@@ -162,7 +163,7 @@ __global__ void parse_write_kernel(ParseGeom g, unsigned long long nseg, const u
       if (bc > 32u) { atomicExch(o.status + 1, 2ull); return; }
       q = p + block_bytes((unsigned)len, bc, g.tags);
     } else {
-      q = p + 4 + (g.tags ? 1 : 0);
+      q = p + 4 + (g.cpu ? 1 : 0) + (g.tags ? 1 : 0);
     }
     if (idx == nb - 1) {
       if (q > lim) { atomicExch(o.status + 1, 3ull); return; }
@@ -174,7 +175,7 @@ __global__ void parse_write_kernel(ParseGeom g, unsigned long long nseg, const u
   }
 }
 
-static unsigned parse_M(int B, bool tags) { return block_bytes((unsigned)B, 32u, tags); }
+static unsigned parse_M(int B, bool tags) { return block_bytes((unsigned)B, 32u, tags) + (B == 1 ? 1u : 0u); }
 
 static void parse_levels(unsigned long long nseg, unsigned long long *cnt, int *nlev) {
   int L = 0;
@@ -200,9 +201,10 @@ size_t parse_scratch_bytes(unsigned long long buf_len, int B, bool tags) {
 
 int parse_stream(szp_b200_ctx *ctx, Arena &A, const unsigned char *d_payload, unsigned long long buf_len,
                  unsigned long long n, const unsigned long long *d_n, int B, bool tags, bool ref_bound,
-                 unsigned long long *d_offs, unsigned long long *d_status) {
+                 unsigned long long *d_offs, unsigned long long *d_status, bool cpu) {
   cudaStream_t s = ctx->stream;
   ParseGeom g;
+  g.cpu = cpu;
   g.p = d_payload;
   g.len = buf_len;
   g.B = B;

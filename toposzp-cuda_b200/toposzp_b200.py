@@ -51,6 +51,9 @@ EXPORTS = [
     "szp_b200_topo_encode_noalloc",
     "szp_b200_topo_check",
     "szp_b200_selftest_bounded_wait",
+    "szp_b200_container_bound",
+    "szp_b200_container_from_streams_dev",
+    "szp_b200_container_decompress_dev",
     "szp_b200_batch_create",
     "szp_b200_batch_destroy",
     "szp_b200_batch_configure",
@@ -171,6 +174,10 @@ def lib():
             "szp_b200_topo_encode_noalloc": (i, [vp, Geom, f, i, vp, sz, C.POINTER(sz), vp]),
             "szp_b200_topo_check": (i, [vp, vp, vp, Geom, f, C.POINTER(TopoReport)]),
             "szp_b200_selftest_bounded_wait": (i, [i, i, C.POINTER(i), C.POINTER(f)]),
+            "szp_b200_container_bound": (sz, [sz, i, i]),
+            "szp_b200_container_from_streams_dev": (i, [vp, vp, sz, vp, sz, Geom, i, sz, i, vp, sz,
+                                                        C.POINTER(sz)]),
+            "szp_b200_container_decompress_dev": (i, [vp, vp, sz, Geom, f, i, vp, vp, i]),
             "szp_b200_batch_create": (vp, [vp, i]),
             "szp_b200_batch_destroy": (None, [vp]),
             "szp_b200_batch_configure": (i, [vp, i, i]),
@@ -429,6 +436,34 @@ class Context:
         if rc:
             raise ToposzpError(last_error())
         return h_out
+
+    def to_container(self, topo, topo_bytes, sort, sort_bytes, shape, block_size, extrema, threads=1):
+        """.SZp container (OpenMP layout, `threads` chunks) of device streams -> uint8 device tensor."""
+        import torch
+        n = int(np.prod(shape))
+        L = lib()
+        out = torch.empty(L.szp_b200_container_bound(n, block_size, threads), dtype=torch.uint8, device=topo.device)
+        nb = C.c_size_t(0)
+        rc = L.szp_b200_container_from_streams_dev(
+            self.ptr, C.c_void_p(topo.data_ptr()), topo_bytes,
+            C.c_void_p(sort.data_ptr()) if sort is not None and sort_bytes else None, sort_bytes,
+            geom_of(shape), block_size, extrema, threads, C.c_void_p(out.data_ptr()), out.numel(), C.byref(nb))
+        if rc:
+            raise ToposzpError(last_error())
+        return out[: nb.value]
+
+    def decompress_container(self, cont, shape, eb: float, block_size: int = 64, postprocess: int = 1,
+                             out=None, types=None):
+        import torch
+        n = int(np.prod(shape))
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device=cont.device)
+        rc = lib().szp_b200_container_decompress_dev(
+            self.ptr, C.c_void_p(cont.data_ptr()), cont.numel(), geom_of(shape), eb, block_size,
+            C.c_void_p(out.data_ptr()), C.c_void_p(types.data_ptr()) if types is not None else None, postprocess)
+        if rc:
+            raise ToposzpError(last_error())
+        return out
 
     def topo_check(self, d_orig, d_dec, shape, eb: float) -> dict:
         """Topology report of a decompressed device field against the original."""
