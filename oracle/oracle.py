@@ -15,7 +15,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libszp_ref.so")
-REF_SRC = os.environ.get("TOPOSZP_REF_SRC", "/root/reference")
+# reference source tree: the build argument, else $TOPOSZP_REF_SRC (no default:
+# without either, an already built _ref/libszp_ref.so is used as it is)
+REF_SRC = os.environ.get("TOPOSZP_REF_SRC")
 
 
 class CP2(C.Structure):
@@ -34,13 +36,16 @@ CP3_DT = np.dtype([("x", "<i4"), ("y", "<i4"), ("z", "<i4"), ("type", "<i4"),
                    ("quantized_bin", "<i4"), ("sort_position", "<i4")])
 
 
-def build(ref: bool = True) -> None:
-    """Compile liboracle.so (always) and the reference library (when the
-    reference sources are present)."""
+def build(ref: bool = True, ref_src: str | None = None) -> None:
+    """Compile liboracle.so (always) and the reference library from the
+    reference sources at ref_src (or $TOPOSZP_REF_SRC) when they are there."""
+    src = ref_src or REF_SRC
     targets = ["oracle"]
-    if ref and os.path.isdir(os.path.join(REF_SRC, "SZp")):
+    args = []
+    if ref and src and os.path.isdir(os.path.join(src, "SZp")):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, "REF=" + REF_SRC] + targets, check=True)
+        args = ["REF=" + src]
+    subprocess.run(["make", "-s", "-C", HERE] + args + targets, check=True)
 
 
 _ora = None
