@@ -459,16 +459,16 @@ def serve_leg(T, dev, nreq=400, slots=4, rate=2000.0, seed=4):
                    edges[k] <= sizes_b[i] <= edges[k + 1] and (k == 9 or sizes_b[i] < edges[k + 1])]
             if not sel:
                 continue
-            st = {}
+            acc = {}
             for i in sel:
                 for name, ms in stage_rows[i]:
-                    st[name] = st.get(name, 0.0) + ms
+                    acc[name] = acc.get(name, 0.0) + ms
             mb = float(sizes_b[sel].sum() / 1e6)
             tsum = float(svc[sel].sum())
             breakdown.append({"op": "compress" if op == "c" else "decompress", "decile": k,
                               "requests": len(sel), "mb": round(mb, 1), "device_s": round(tsum, 4),
                               "gbs": round(mb / 1e3 / tsum, 2) if tsum > 0 else None,
-                              "stages_ms": {kk: round(v, 2) for kk, v in sorted(st.items(), key=lambda x: -x[1])}})
+                              "stages_ms": {kk: round(v, 2) for kk, v in sorted(acc.items(), key=lambda x: -x[1])}})
     t = 0.0
     plat = np.zeros(nreq)
     for i in range(nreq):

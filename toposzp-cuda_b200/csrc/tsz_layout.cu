@@ -145,7 +145,7 @@ static int detect_chunks(szp_b200_ctx *ctx, Arena &A, const unsigned char *cmp, 
   if (cuda_fail(cudaMemcpyAsync(tab.data(), cmp, (size_t)tmax * 8, cudaMemcpyDeviceToHost, s), "D2H") ||
       cuda_fail(cudaStreamSynchronize(s), "table"))
     return -1;
-  auto try_T = [&](int T, bool *ok) -> int {
+  auto try_T = [&](int T, unsigned long long bound, bool *ok) -> int {
     *ok = false;
     const unsigned long long hdr = (unsigned long long)T * 8;
     if (hdr >= bound) return 0;
@@ -168,12 +168,15 @@ static int detect_chunks(szp_b200_ctx *ctx, Arena &A, const unsigned char *cmp, 
         if (tab[k] > maxc || tab[k] < tab[k - 1]) { valid = false; break; }
       if (!valid) break;
       bool ok = false;
-      if (try_T(T, &ok)) return -1;
+      if (try_T(T, bound, &ok)) return -1;
       if (ok) return T;
     }
   }
+  // No candidate validated: the reference then takes one thread without a
+  // walk (so a single chunk longer than its validation bound is read as
+  // well); here that chunk is walked inside the stream's own length.
   bool ok = false;
-  if (try_T(1, &ok)) return -1;
+  if (try_T(1, len, &ok)) return -1;
   return ok ? 1 : 0;
 }
 
