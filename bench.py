@@ -412,7 +412,9 @@ def serve_leg(T, dev, nreq=400, slots=4, rate=2000.0, seed=4):
                 topo, tn, sort, sn, eb = pre[sp[1]]
                 arr[j] = srv.decompress_request(topo, tn, sort if sn else None, sn, dims, eb, sp[2], 1)
         return arr
-    # warm-up: autotuning and workspace growth in every slot
+    # warm-up: every worker's workspace sized for the largest field (no
+    # allocation while serving), autotuning of the batch compressors
+    srv.reserve(max(int(np.prod(dims)) for dims, _ in pool))
     warm = list(range(min(nreq, 160)))
     srv.run_trace(requests(warm))
     srv.run_trace(requests(warm))

@@ -382,6 +382,11 @@ typedef struct szp_b200_server szp_b200_server;
 SZP_B200_API szp_b200_server *szp_b200_server_create(const szp_b200_server_config *cfg);
 SZP_B200_API void szp_b200_server_destroy(szp_b200_server *s);
 SZP_B200_API double szp_b200_server_now(szp_b200_server *s);
+/* Grows every worker's device workspace for requests of up to max_elements
+ * elements, so that serving them allocates nothing (an allocation while
+ * other workers run would stall the device for all of them).  Call it while
+ * no request is in flight.  Returns 0 on success. */
+SZP_B200_API int szp_b200_server_reserve(szp_b200_server *s, size_t max_elements);
 SZP_B200_API int szp_b200_server_submit(szp_b200_server *s, szp_b200_request *r);
 /* 0 when r finished within timeout_s, 1 on timeout */
 SZP_B200_API int szp_b200_server_wait(szp_b200_server *s, szp_b200_request *r, double timeout_s);

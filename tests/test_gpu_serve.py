@@ -152,3 +152,37 @@ def test_poisson_trace(T):
     lat = np.array([r.t_done - r.t_arrival for r in arr])
     assert (lat > 0).all() and np.isfinite(lat).all()
     srv.close()
+
+
+def test_large_compressions_run_alone_and_match(T):
+    """Compressions of at least 2^21 elements take the fused single-field path
+    inside the server (not the batched one); their streams equal the plain
+    call's, alone and beside small merged requests, after a workspace
+    reserve."""
+    import torch
+    L = T.lib()
+    big = (160, 128, 128)
+    d = torch.from_numpy(synth.small_field(big, seed=42, kind="band").reshape(-1).copy()).cuda()
+    ctx = T.Context()
+    ref_t, ref_s, _, ref_sz = ctx.compress(d, big, 1e-4, 64, index=False)
+    ref = (ref_t[:ref_sz.topo_bytes].cpu().numpy().tobytes(), ref_s[:ref_sz.sort_bytes].cpu().numpy().tobytes())
+    ctx.close()
+    srv = T.Server(slots=3, max_batch=8, block_size=64)
+    srv.reserve(d.numel())
+    spec = []
+    n = d.numel()
+    for k in range(2):
+        tb = torch.empty(L.szp_b200_topo_bound(n, 64), dtype=torch.uint8, device="cuda")
+        sb = torch.empty(L.szp_b200_sort_bound(n, 64), dtype=torch.uint8, device="cuda")
+        spec.append(("c", big, d, 1e-4, False, tb, sb))
+    small, keep = build_mix(T, seed=9)
+    arr = to_requests(T, srv, spec + small)
+    srv.run_trace(arr)
+    for k in range(2):
+        r = arr[k]
+        assert r.status == 0, r.message
+        got = (spec[k][5][:r.sizes.topo_bytes].cpu().numpy().tobytes(),
+               spec[k][6][:r.sizes.sort_bytes].cpu().numpy().tobytes())
+        assert got == ref
+    assert all(arr[i].status == 0 for i in range(len(arr)))
+    srv.close()

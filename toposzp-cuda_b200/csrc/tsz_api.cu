@@ -58,6 +58,23 @@ bool geom_elements(const szp_b200_geom &g, unsigned long long *n, Geom *out) {
   return true;
 }
 
+static size_t stream_bound(unsigned long long n, int B, bool tags);
+
+int ctx_reserve_for(szp_b200_ctx *ctx, unsigned long long n, int B) {
+  DeviceGuard dg(ctx);
+  if (!ctx || n == 0 || B <= 0) { set_error("ctx_reserve_for: invalid arguments"); return -1; }
+  const unsigned long long nb = (n + B - 1) / B;
+  // the largest scratch of a fused compression and of a fused decompression
+  // with post-processing and device stream parsing
+  const size_t comp = a256(n * 8) + a256(n * 4) + a256((nb / enc_tile_blocks(B) + 2) * sizeof(TileDesc)) * 2 +
+                      rank_scratch_bytes(n, ctx->sm_count) + 8192;
+  const size_t dec = post_scratch_bytes(n) + a256(n * 4) + a256(n) + 8192 + a256(2 * nb * 8) +
+                     parse_scratch_bytes(stream_bound(n, B, true) - 8, B, true) +
+                     parse_scratch_bytes(stream_bound(n, B, false) - 8, B, false);
+  if (!ctx->scratch.reserve(comp > dec ? comp : dec)) return -1;
+  return post_words(ctx, n) ? 0 : -1;
+}
+
 static bool check_block_size(int B, const char *fn) {
   if (B <= 0 || B > kMaxBlockSize) {
     set_error("%s: blockSize %d out of range [1, %d]", fn, B, kMaxBlockSize);

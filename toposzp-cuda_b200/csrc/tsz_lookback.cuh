@@ -106,20 +106,25 @@ namespace tsz {
 // CTA-wide look-back: all WARPS * 32 threads of the CTA call it after the
 // tile's aggregate has been published.  Each round inspects one predecessor
 // per thread, so a walk back over P in-flight tiles takes about P / (WARPS *
-// 32) rounds instead of P / 32.
+// 32) rounds instead of P / 32.  One CTA barrier per round: every warp sums
+// its own predecessors up to its nearest inclusive one and posts (nearest
+// inclusive, sums) to a double-buffered slot; after the barrier every thread
+// adds the posts of the warps up to the first warp holding an inclusive
+// prefix (round r writes buffer r & 1, which round r + 2 may overwrite only
+// after every thread has passed round r + 1's barrier).
 // spin_limit: polls of one predecessor before the wait gives up (0: kSpinLimit)
 template <int WARPS = kWarps>
 __device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long long agg_bytes,
                                       unsigned long long agg_cnt, int *err, int spin_limit = 0) {
   const int limit = spin_limit > 0 ? spin_limit : kSpinLimit;
-  __shared__ unsigned s_first[WARPS];
-  __shared__ unsigned long long s_b[WARPS], s_c[WARPS];
+  __shared__ unsigned s_first[2][WARPS];
+  __shared__ unsigned long long s_b[2][WARPS], s_c[2][WARPS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   Prefix ex{0ull, 0ull};
   if (t == 0) return ex;
   long long base = t - 1;
   bool timed_out = false;
-  while (true) {
+  for (int r = 0;; r ^= 1) {
     const long long idx = base - (long long)threadIdx.x;
     unsigned long long st = (2ull << kStatShift);
     if (idx >= 0) {
@@ -132,16 +137,12 @@ __device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long
       }
     }
     unsigned long long flag = st >> kStatShift;
-    if (flag == 0ull) flag = 2ull;
-    // nearest predecessor (smallest thread index) holding an inclusive prefix
+    if (flag == 0ull) flag = 2ull;   // timed out: an empty inclusive value
+    // this warp's nearest inclusive predecessor (smallest lane)
     const unsigned wm = __ballot_sync(0xffffffffu, flag == 2ull);
-    if (lane == 0) s_first[warp] = wm ? (unsigned)(warp * 32 + __ffs(wm) - 1) : 0xffffffffu;
-    __syncthreads();
-    unsigned first = 0xffffffffu;
-#pragma unroll
-    for (int w = 0; w < WARPS; w++) first = min(first, s_first[w]);
+    const int wfirst = wm ? (__ffs(wm) - 1) : 32;
     unsigned long long b = 0, c = 0;
-    if ((unsigned)threadIdx.x <= first && idx >= 0 && (st >> kStatShift) != 0ull) {
+    if (lane <= wfirst && idx >= 0 && (st >> kStatShift) != 0ull) {
       b = st & kByteMask;
       c = (flag == 2ull) ? ld_relaxed_u64(&desc[idx].inc_cnt) : ld_relaxed_u64(&desc[idx].agg_cnt);
     }
@@ -150,12 +151,22 @@ __device__ inline Prefix lookback_cta(TileDesc *desc, long long t, unsigned long
       b += __shfl_xor_sync(0xffffffffu, b, o);
       c += __shfl_xor_sync(0xffffffffu, c, o);
     }
-    if (lane == 0) { s_b[warp] = b; s_c[warp] = c; }
+    if (lane == 0) {
+      s_first[r][warp] = wm ? 1u : 0u;
+      s_b[r][warp] = b;
+      s_c[r][warp] = c;
+    }
     __syncthreads();
+    bool found = false;
 #pragma unroll
-    for (int w = 0; w < WARPS; w++) { ex.bytes += s_b[w]; ex.cnt += s_c[w]; }
-    __syncthreads();
-    if (first != 0xffffffffu) break;
+    for (int w = 0; w < WARPS; w++) {
+      if (!found) {
+        ex.bytes += s_b[r][w];
+        ex.cnt += s_c[r][w];
+        found = s_first[r][w] != 0u;
+      }
+    }
+    if (found) break;
     base -= WARPS * 32;
   }
   if (timed_out) atomicExch(err, kErrLookbackTimeout);

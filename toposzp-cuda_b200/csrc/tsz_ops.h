@@ -81,4 +81,8 @@ int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, size_t t
                         bool ref_bound, bool *parse_failed, cudaEvent_t sort_ready = nullptr,
                         bool cpu_layout = false, unsigned long long sort_count = ~0ull);
 
+// Grows a workspace so that compressing or decompressing (with
+// post-processing) a field of n elements allocates nothing more.
+int ctx_reserve_for(szp_b200_ctx *ctx, unsigned long long n, int B);
+
 }  // namespace tsz

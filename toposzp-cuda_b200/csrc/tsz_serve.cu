@@ -113,10 +113,44 @@ static int compress_group(Slot &sl, szp_b200_request **rs, int count) {
   return rc;
 }
 
+// A compression of at least this many elements fills the GPU by itself: it
+// runs alone through the fused single-field path (the blockSize-64 encoder
+// and the single-field rank), and smaller ones are merged into batched
+// launches behind a small head.
+constexpr size_t kAloneElems = (size_t)1 << 21;
+
+static int compress_alone(Slot &sl, szp_b200_request *r) {
+  float eb = r->errBound;
+  if (r->rel) {
+    // the batch compressor resolves relative bounds on the device; one field
+    // alone goes through it as a batch of one
+    return 1;
+  }
+  szp_b200_sizes sz{};
+  const int rc = szp_b200_topo_compress_dev(sl.ctx, r->d_data, r->geom, eb, r->blockSize, r->d_topo, r->d_sort,
+                                            nullptr, &sz);
+  if (rc == 0) {
+    r->status = 0;
+    r->sizes = sz;
+    r->abs_eb = eb;
+    r->message[0] = 0;
+  }
+  return rc ? -1 : 0;
+}
+
 static void run_group(szp_b200_server *S, Slot &sl, std::vector<Item> &grp) {
   const double ts = S->now();
   for (auto &it : grp) it.r->t_start = ts;
   szp_b200_request *head = grp[0].r;
+  if (head->op == SZP_B200_OP_COMPRESS && grp.size() == 1 && elems_of(head->geom) >= kAloneElems &&
+      head->blockSize == 64) {
+    const int rc = compress_alone(sl, head);
+    if (rc <= 0) {
+      if (rc < 0) fail_request(head, szp_b200_last_error());
+      head->t_done = S->now();
+      return;
+    }
+  }
   if (head->op == SZP_B200_OP_COMPRESS) {
     std::vector<szp_b200_request *> rs;
     for (auto &it : grp) rs.push_back(it.r);
@@ -165,11 +199,13 @@ static void worker_main(szp_b200_server *S, int w) {
       grp.push_back(S->q.front());
       S->q.pop_front();
       size_t bytes = grp[0].cost;
-      if (grp[0].r->op == SZP_B200_OP_COMPRESS) {
-        // continuous batching: compressions queued behind the head join its launch
+      if (grp[0].r->op == SZP_B200_OP_COMPRESS && elems_of(grp[0].r->geom) < kAloneElems) {
+        // continuous batching: small compressions queued behind a small head
+        // join its launch (large ones run alone on the fused path)
         for (auto it = S->q.begin(); it != S->q.end() && (int)grp.size() < S->cfg.max_batch;) {
           if (it->r->op == SZP_B200_OP_COMPRESS && it->r->blockSize == grp[0].r->blockSize &&
-              bytes + it->cost <= batch_cap && S->inflight_bytes + bytes + it->cost <= S->cfg.hbm_budget) {
+              elems_of(it->r->geom) < kAloneElems && bytes + it->cost <= batch_cap &&
+              S->inflight_bytes + bytes + it->cost <= S->cfg.hbm_budget) {
             bytes += it->cost;
             grp.push_back(*it);
             it = S->q.erase(it);
@@ -182,7 +218,7 @@ static void worker_main(szp_b200_server *S, int w) {
       S->inflight += (int)grp.size();
       if (S->inflight_bytes > S->max_inflight_bytes) S->max_inflight_bytes = S->inflight_bytes;
       if (S->inflight > S->max_concurrent) S->max_concurrent = S->inflight;
-      if (grp[0].r->op == SZP_B200_OP_COMPRESS) {
+      if (grp[0].r->op == SZP_B200_OP_COMPRESS && elems_of(grp[0].r->geom) < kAloneElems) {
         S->batches++;
         S->batched_requests += grp.size();
       }
@@ -259,6 +295,18 @@ void szp_b200_server_destroy(szp_b200_server *S) {
 }
 
 double szp_b200_server_now(szp_b200_server *S) { return S ? S->now() : 0.0; }
+
+int szp_b200_server_reserve(szp_b200_server *S, size_t max_elements) {
+  clear_error();
+  if (!S) { set_error("null argument"); return -1; }
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->inflight || !S->q.empty()) { set_error("szp_b200_server_reserve: requests are in flight"); return -1; }
+  }
+  for (auto &sl : S->slots)
+    if (ctx_reserve_for(sl.ctx, max_elements, S->cfg.blockSize)) return -1;
+  return 0;
+}
 
 int szp_b200_server_submit(szp_b200_server *S, szp_b200_request *r) {
   clear_error();

@@ -63,6 +63,7 @@ EXPORTS = [
     "szp_b200_server_create",
     "szp_b200_server_destroy",
     "szp_b200_server_now",
+    "szp_b200_server_reserve",
     "szp_b200_server_submit",
     "szp_b200_server_wait",
     "szp_b200_server_drain",
@@ -187,6 +188,7 @@ def lib():
             "szp_b200_server_create": (vp, [C.POINTER(ServerConfig)]),
             "szp_b200_server_destroy": (None, [vp]),
             "szp_b200_server_now": (C.c_double, [vp]),
+            "szp_b200_server_reserve": (i, [vp, sz]),
             "szp_b200_server_submit": (i, [vp, C.POINTER(Request)]),
             "szp_b200_server_wait": (i, [vp, C.POINTER(Request), C.c_double]),
             "szp_b200_server_drain": (i, [vp, C.c_double]),
@@ -581,6 +583,11 @@ class Server:
             self.close()
         except Exception:
             pass
+
+    def reserve(self, max_elements: int):
+        """Grows every worker's workspace for requests of up to max_elements."""
+        if lib().szp_b200_server_reserve(self.ptr, int(max_elements)):
+            raise ToposzpError(last_error())
 
     def compress_request(self, d_data, shape, err, rel, d_topo, d_sort) -> Request:
         r = Request()
