@@ -365,7 +365,7 @@ def serve_pool(count=32, seed=4):
     return pool
 
 
-def serve_leg(T, dev, nreq=400, slots=4, rate=2000.0, seed=4):
+def serve_leg(T, dev, nreq=600, slots=4, rate=2000.0, seed=4):
     """Served mode against back-to-back plain calls on the same requests.
     Served: requests submitted at their Poisson arrival times to the server
     (continuous batching, HBM budget 120 GiB); latency = completion - arrival.
@@ -512,6 +512,8 @@ def parse():
     ap.add_argument("--no-e2e-pipelined", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-vs-plain leg")
+    ap.add_argument("--serve-requests", type=int, default=600, help="requests of the served leg")
+    ap.add_argument("--serve-slots", type=int, default=4, help="server worker slots")
     return ap.parse_args()
 
 
@@ -769,7 +771,7 @@ def main():
 
     served = None
     if not args.no_serve:
-        served = serve_leg(T, dev)
+        served = serve_leg(T, dev, nreq=args.serve_requests, slots=args.serve_slots)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
