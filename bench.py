@@ -697,6 +697,19 @@ def main():
 
     # check the last output against the error bound (cheap, after timing)
     err = (out - d_field).abs().max().item()
+    # topology of the last output against the original, on the device, with
+    # the reference drivers' acceptance rule (max error <= 2 eb and more than
+    # 90 % of the critical points preserved)
+    rep = ctx.topo_check(d_field, out, dims, eb)
+    ncp = max(1, rep["orig_cps"][0])
+    topology = {"orig_cps": rep["orig_cps"][0], "preserved": rep["preserved"],
+                "cp_preserved_frac": rep["preserved"] / ncp, "lost": rep["lost"], "changed": rep["changed"],
+                "false_negatives": rep["lost"] + rep["changed"], "false_positives": rep["new_cps"],
+                "order_pairs": rep["pairs"][0], "order_violations": rep["violations"][0],
+                "order_violations_at_cps": rep["violations"][1],
+                "order_violations_at_extrema": rep["violations"][3],
+                "max_err_over_eb": rep["max_err"] / eb, "over_2eb": rep["over_2eb"],
+                "accepted": bool(rep["max_err"] <= 2 * eb and rep["preserved"] > 0.9 * ncp)}
 
     stages = {k: statistics.mean(v) for k, v in stage_acc.items()}
     peak, peak_kind = peaks()
@@ -792,6 +805,7 @@ def main():
                        "topo_bytes": s_topo, "sort_bytes": s_sort,
                        "compression_ratio": 4.0 * n / (s_topo + s_sort),
                        "max_abs_err_over_eb": err / eb},
+            "topology": topology,
             "clocks": clk.summary(),
             "gpu_launches": launches,
             "stages_ms": stages,
