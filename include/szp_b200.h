@@ -99,6 +99,15 @@ SZP_B200_API unsigned char *szp_cuda_float_compress_topology_3d(
     CriticalPoint3D *critical_points, int critical_count,
     int d1, int d2, int d3);
 
+/* replaces SZp/include/szp_cuda_topology_3d.cuh:34-38 (szp_cuda_topology_3d.cu:1066):
+ * fp64 field, double quantization, three saddle-repair passes in q-space,
+ * the fp32 path's stream format ([u64 0][blocks with 2-bit tags]). */
+SZP_B200_API unsigned char *szp_cuda_double_compress_topology_3d(
+    double *oriData, size_t *outSize, double absErrBound,
+    size_t nbEle, int blockSize,
+    CriticalPoint3D *critical_points, int critical_count,
+    int d1, int d2, int d3);
+
 /* replaces SZp/include/szp_cuda_decompress.cuh:63-65 (szp_cuda_decompress.cu:1074) */
 SZP_B200_API void szp_cuda_float_decompress_randomaccess_topology_preserved(
     float **newData, size_t nbEle, float absErrBound, int blockSize,
@@ -267,6 +276,22 @@ SZP_B200_API int szp_b200_container_from_streams_dev(szp_b200_ctx *ctx, const un
 SZP_B200_API int szp_b200_container_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_in, size_t in_bytes,
                                                    szp_b200_geom geom, float absErrBound, int blockSize,
                                                    float *d_out, unsigned char *d_types, int postprocess);
+
+/* The fp64 3D compression on device memory: d_data (nd 3 geometry), the
+ * critical points on the device (d_cps, critical_count records; null when 0),
+ * `passes` saddle-repair passes (the reference runs 3; 0..64).  Writes the
+ * stream to d_out (out_cap >= szp_b200_topo_bound(n, blockSize)) and its
+ * length to *out_len; with d_q non-null the repaired integers go there
+ * (n ints) instead of workspace scratch.  Returns 0, or -1 with
+ * szp_b200_last_error(). */
+SZP_B200_API int szp_b200_double_compress_topology_3d_dev(szp_b200_ctx *ctx, const double *d_data,
+                                                          szp_b200_geom geom, double absErrBound,
+                                                          int blockSize, const CriticalPoint3D *d_cps,
+                                                          size_t critical_count, int passes,
+                                                          unsigned char *d_out, size_t out_cap,
+                                                          size_t *out_len, int *d_q);
+/* Device scratch the call above takes from the workspace. */
+SZP_B200_API size_t szp_b200_f64_topo_scratch_bytes(size_t n, size_t critical_count, int blockSize);
 
 /* Bounded-wait self-test (no reference counterpart).  Every device wait of
  * the library gives up after a poll limit and reports an error instead of

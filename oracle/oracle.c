@@ -19,13 +19,15 @@
 /* ------------------------------------------------------------------ */
 
 /* (int)((double)x * inv) as the CUDA path evaluates it
- * (SZp/src/szp_cuda_topology.cu:547,592): truncation toward zero, with the
- * device conversion's saturation and NaN -> 0 (cvt.rzi.s32.f64).  For values
- * inside the int range this is identical to the host cast
- * (SZp/src/szp_float.cc:1212). */
+ * (SZp/src/szp_cuda_topology.cu:547,592): truncation toward zero, values
+ * beyond the int range saturate, and NaN converts to INT_MIN -- the outputs
+ * of the reference's own CUDA build on sm_100a for +-inf, +-1e300, values just
+ * outside the range and NaN (the special_20x21x22 case of
+ * tests/golden/f64_topo.json).  For values inside the int range this is
+ * identical to the host cast (SZp/src/szp_float.cc:1212). */
 static int trunc_sat(double v)
 {
-    if (v != v) return 0;
+    if (v != v) return (-2147483647 - 1);
     if (v >= 2147483647.0) return 2147483647;
     if (v <= -2147483648.0) return (-2147483647 - 1);
     return (int)v;
@@ -360,6 +362,85 @@ size_t ora_encode_ints(const int *v, size_t n, int B, int cpu_layout, uint8_t *o
         size_t m = (n - s < (size_t)B) ? n - s : (size_t)B;
         off += encode_block(v + s, m, NULL, cpu_layout, out + off);
     }
+    return off;
+}
+
+/* ------------------------------------------------------------------ */
+/* fp64 3D topology compression                                        */
+/* ------------------------------------------------------------------ */
+
+/* Integer arithmetic of the saddle repair wraps (c - 1 at INT_MIN). */
+static int wrap_add(int a, int d) { return (int)((unsigned)a + (unsigned)d); }
+
+/* One repair pass over the interior saddles (type 3), all reads from the
+ * snapshot src, writes into dst (SZp/src/szp_cuda_topology_3d.cu:736-826).
+ * A saddle that is still high along one axis and low along another keeps its
+ * value; otherwise c, c - 1, c + 1 are tried in that order, and the first
+ * that is high along >= 1 axis, low along >= 1 axis and leaves every
+ * neighbouring maximum above it and every neighbouring minimum below it is
+ * written.  Interior: 1 <= x <= d1-2 (y, z alike); a grid with an axis below
+ * 3 has none.  Points whose +x neighbour lies at or beyond n are skipped. */
+static void fix_saddles_pass(const int *src, int *dst, const uint8_t *ty, size_t n, int d1, int d2, int d3)
+{
+    if (d1 < 3 || d2 < 3 || d3 < 3) return;
+    const size_t pl = (size_t)d2 * d3;
+    const long long st[6] = {-(long long)pl, (long long)pl, -(long long)d3, (long long)d3, -1, 1};
+    for (int x = 1; x <= d1 - 2; x++)
+        for (int y = 1; y <= d2 - 2; y++)
+            for (int z = 1; z <= d3 - 2; z++) {
+                size_t p = (size_t)x * pl + (size_t)y * d3 + z;
+                if (p + pl >= n || ty[p] != 3) continue;
+                int c = src[p], v[6], hi[3], lo[3];
+                for (int k = 0; k < 6; k++) v[k] = src[(size_t)((long long)p + st[k])];
+                int nh = 0, nl = 0;
+                for (int a = 0; a < 3; a++) {
+                    hi[a] = v[2 * a] > v[2 * a + 1] ? v[2 * a] : v[2 * a + 1];
+                    lo[a] = v[2 * a] < v[2 * a + 1] ? v[2 * a] : v[2 * a + 1];
+                    nh += c > hi[a];
+                    nl += c < lo[a];
+                }
+                if (nh >= 1 && nl >= 1) continue;
+                const int tries[3] = {0, -1, 1};
+                for (int t = 0; t < 3; t++) {
+                    int tv = wrap_add(c, tries[t]);
+                    int th = 0, tl = 0;
+                    for (int a = 0; a < 3; a++) { th += tv > hi[a]; tl += tv < lo[a]; }
+                    if (th < 1 || tl < 1) continue;
+                    int ok = 1;
+                    for (int k = 0; k < 6; k++) {
+                        uint8_t tk = ty[(size_t)((long long)p + st[k])];
+                        if (tk == 1 && v[k] <= tv) ok = 0;
+                        if (tk == 2 && v[k] >= tv) ok = 0;
+                    }
+                    if (ok) { dst[p] = tv; break; }
+                }
+            }
+}
+
+/* q = (int)(x * (1/eb)) in double (SZp/src/szp_cuda_topology_3d.cu:641-646),
+ * `passes` snapshot repair passes (three in the reference, :1125-1145), then
+ * the topology block layout over the ints with the 2-bit tags
+ * (:836-958, header :1171-1174): [u64 0][blocks].  Writes q after repair to
+ * q_out when it is not NULL. */
+size_t ora_double_compress_topo_3d(const double *d, size_t n, double eb, int B, const uint8_t *types,
+                                   int d1, int d2, int d3, int passes, int *q_out, uint8_t *out)
+{
+    double inv = 1.0 / eb;
+    int *q = (int *)malloc(n * sizeof(int));
+    int *src = (int *)malloc(n * sizeof(int));
+    for (size_t i = 0; i < n; i++) q[i] = trunc_sat(d[i] * inv);
+    for (int p = 0; p < passes; p++) {
+        memcpy(src, q, n * sizeof(int));
+        fix_saddles_pass(src, q, types, n, d1, d2, d3);
+    }
+    memset(out, 0, 8);
+    size_t off = 8;
+    for (size_t s = 0; s < n; s += (size_t)B) {
+        size_t m = (n - s < (size_t)B) ? n - s : (size_t)B;
+        off += encode_block(q + s, m, types + s, 0, out + off);
+    }
+    if (q_out) memcpy(q_out, q, n * sizeof(int));
+    free(q); free(src);
     return off;
 }
 

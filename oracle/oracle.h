@@ -51,6 +51,8 @@ size_t ora_extract_sp_3d(const ora_cp3 *cp, size_t k, int *sp);
 size_t ora_encode_topo(const float *data, size_t n, float eb, int B,
                        const uint8_t *types, int cpu_layout, uint8_t *out);
 size_t ora_encode_ints(const int *v, size_t n, int B, int cpu_layout, uint8_t *out);
+size_t ora_double_compress_topo_3d(const double *d, size_t n, double eb, int B, const uint8_t *types,
+                                   int d1, int d2, int d3, int passes, int *q_out, uint8_t *out);
 size_t ora_topo_bound(size_t n, int B);
 size_t ora_ints_bound(size_t n, int B);
 

@@ -15,6 +15,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libszp_ref.so")
+# the reference's CUDA 3D topology library (runs on a GPU; fixture generation only)
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libszp_ref_cuda3d.so")
 # reference source tree: the build argument, else $TOPOSZP_REF_SRC (no default:
 # without either, an already built _ref/libszp_ref.so is used as it is)
 REF_SRC = os.environ.get("TOPOSZP_REF_SRC")
@@ -43,7 +45,7 @@ def build(ref: bool = True, ref_src: str | None = None) -> None:
     targets = ["oracle"]
     args = []
     if ref and src and os.path.isdir(os.path.join(src, "SZp")):
-        targets.append("ref")
+        targets += ["ref", "refcuda"]
         args = ["REF=" + src]
     subprocess.run(["make", "-s", "-C", HERE] + args + targets, check=True)
 
@@ -77,6 +79,7 @@ def lib():
             "ora_extract_sp_3d": (sz, [vp, sz, vp]),
             "ora_encode_topo": (sz, [vp, sz, f, i, vp, i, vp]),
             "ora_encode_ints": (sz, [vp, sz, i, i, vp]),
+            "ora_double_compress_topo_3d": (sz, [vp, sz, d, i, vp, i, i, i, i, vp, vp]),
             "ora_topo_bound": (sz, [sz, i]),
             "ora_ints_bound": (sz, [sz, i]),
             "ora_decode_topo": (i, [vp, sz, sz, f, i, vp, vp, C.POINTER(sz)]),
@@ -222,6 +225,22 @@ def encode_topo(data: np.ndarray, eb: float, B: int, types=None, cpu_layout=Fals
     t = None if types is None else np.ascontiguousarray(types, dtype=np.uint8).reshape(-1)
     m = lib().ora_encode_topo(_p(d), n, eb, B, _p(t), int(cpu_layout), _p(out))
     return out[:m].tobytes()
+
+
+def double_compress_topo_3d(data: np.ndarray, eb: float, B: int, types, dims, passes: int = 3,
+                            with_q: bool = False):
+    """fp64 3D topology stream: double quantization, `passes` saddle-repair
+    passes in q-space, int blocks with 2-bit tags (CUDA layout).  With with_q,
+    also returns the repaired ints."""
+    d = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)
+    n = d.size
+    t = np.ascontiguousarray(types, dtype=np.uint8).reshape(-1)
+    assert t.size == n
+    out = np.zeros(lib().ora_topo_bound(n, B), dtype=np.uint8)
+    q = np.zeros(n, dtype=np.int32)
+    m = lib().ora_double_compress_topo_3d(_p(d), n, float(eb), B, _p(t), dims[0], dims[1], dims[2],
+                                          passes, _p(q), _p(out))
+    return (out[:m].tobytes(), q) if with_q else out[:m].tobytes()
 
 
 def encode_ints(v: np.ndarray, B: int, cpu_layout=False) -> bytes:

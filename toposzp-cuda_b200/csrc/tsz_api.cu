@@ -88,6 +88,18 @@ static size_t stream_bound(unsigned long long n, int B, bool tags) {
   return 8 + nb * (size_t)max_block_bytes((uint32_t)B, tags) + 64;
 }
 
+size_t topo_stream_bound(unsigned long long n, int B) { return stream_bound(n, B, true); }
+
+bool valid_block_size(int B, const char *fn) { return check_block_size(B, fn); }
+
+cudaError_t launch_mark_types(const int *d_cps, int stride, long long count, const Geom &g, unsigned long long n,
+                              unsigned char *d_types, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)((count + 255) / 256);
+  mark_types_kernel<<<blocks, 256, 0, s>>>(d_cps, stride, count, g.nd, g.d1, g.d2, g.d3, n, d_types);
+  return cudaGetLastError();
+}
+
 int encode_pass(szp_b200_ctx *ctx, int mode, const float *d_data, const int *d_ints,
                 const unsigned char *d_types, unsigned long long n, int B, float eb,
                 const Geom &g, unsigned char *d_stream, unsigned long long stream_cap,

@@ -76,8 +76,9 @@ encode_kernel(EncArgs a) {
         int qv = 0;
         uint32_t tv = 0;
         if (in) {
-          if (MODE == kEncInts) {
+          if (MODE == kEncInts || MODE == kEncIntTypes) {
             qv = a.ints[base + j];
+            if (MODE == kEncIntTypes) tv = (uint32_t)(a.types[base + j] & 3u);
           } else {
             const float x = a.data[base + j];
             qv = quantize(x, a.inv);
@@ -582,10 +583,12 @@ cudaError_t launch_encode(int mode, const EncArgs &a, cudaStream_t s, int grid) 
   if (a.B <= 256) {
     if (mode == kEncClassify) return launch_enc2_mode<kEncClassify>(a, s, grid);
     if (mode == kEncTypes) return launch_enc2_mode<kEncTypes>(a, s, grid);
+    if (mode == kEncIntTypes) return launch_enc2_mode<kEncIntTypes>(a, s, grid);
     return launch_enc2_mode<kEncInts>(a, s, grid);
   }
   if (mode == kEncClassify) return launch_enc_mode<kEncClassify>(a, s, grid);
   if (mode == kEncTypes) return launch_enc_mode<kEncTypes>(a, s, grid);
+  if (mode == kEncIntTypes) return launch_enc_mode<kEncIntTypes>(a, s, grid);
   return launch_enc_mode<kEncInts>(a, s, grid);
 }
 

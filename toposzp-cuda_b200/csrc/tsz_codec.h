@@ -4,13 +4,14 @@
 
 namespace tsz {
 
-enum EncMode { kEncClassify = 0, kEncTypes = 1, kEncInts = 2 };
+// kEncIntTypes: int values with per-element 2-bit tags (pre-quantized fields)
+enum EncMode { kEncClassify = 0, kEncTypes = 1, kEncInts = 2, kEncIntTypes = 3 };
 enum CpMode { kCpNone = 0, kCpRecords = 1, kCpPairs = 2 };
 
 struct EncArgs {
   const float *data;            // float field (kEncClassify / kEncTypes)
-  const int *ints;              // int values (kEncInts)
-  const unsigned char *types;   // per-element types 0..3 (kEncTypes)
+  const int *ints;              // int values (kEncInts / kEncIntTypes)
+  const unsigned char *types;   // per-element types 0..3 (kEncTypes / kEncIntTypes)
   unsigned long long n;
   int B;
   float eb;

@@ -198,6 +198,22 @@ struct EncShared {
   unsigned tile_bytes, tile_cps, tile_ext;
 };
 
+// 2-bit tags of nv (1..8) consecutive elements from a byte-per-element
+// type array, element t in bits 2t..2t+1.
+__device__ __forceinline__ unsigned load_type_octet(const unsigned char *__restrict__ ty, long long i0, int nv) {
+  unsigned types = 0;
+  if (nv == 8 && ((reinterpret_cast<uintptr_t>(ty + i0) & 7) == 0)) {
+    const unsigned long long w = __ldg(reinterpret_cast<const unsigned long long *>(ty + i0));
+#pragma unroll
+    for (int t = 0; t < 8; t++) types |= (unsigned)((w >> (8 * t)) & 3u) << (2 * t);
+  } else {
+#pragma unroll
+    for (int t = 0; t < 8; t++)
+      if (t < nv) types |= (unsigned)(ty[i0 + t] & 3u) << (2 * t);
+  }
+  return types;
+}
+
 // Per-thread values of a tile that the record mode of phase 6 reads after
 // the look-back (only the unpipelined path keeps them).
 struct EncRegs {
@@ -238,7 +254,7 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
     unsigned types = 0;
 #pragma unroll
     for (int t = 0; t < 8; t++) { x[t] = 0.f; q[t] = 0; }
-    if (MODE == kEncInts) {
+    if (MODE == kEncInts || MODE == kEncIntTypes) {
       if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.ints + i0) & 15) == 0)) {
         const int4 u = __ldg(reinterpret_cast<const int4 *>(a.ints + i0));
         const int4 w = __ldg(reinterpret_cast<const int4 *>(a.ints + i0) + 1);
@@ -247,6 +263,7 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
 #pragma unroll
         for (int t = 0; t < 8; t++) if (t < nv) q[t] = __ldg(a.ints + i0 + t);
       }
+      if (MODE == kEncIntTypes && nv > 0) types = load_type_octet(a.types, i0, nv);
     } else {
       unsigned inter = 0;
       float ma[8], pa[8], mb[8], pb[8];
@@ -266,15 +283,7 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
       if (MODE == kEncClassify) {
         if (nv > 0) types = classify_octet(a.data, n, i0, nv, x, a.g, inter, ma, pa, mb, pb);
       } else if (nv > 0) {
-        if (nv == 8 && ((reinterpret_cast<uintptr_t>(a.types + i0) & 7) == 0)) {
-          const unsigned long long w = __ldg(reinterpret_cast<const unsigned long long *>(a.types + i0));
-#pragma unroll
-          for (int t = 0; t < 8; t++) types |= (unsigned)((w >> (8 * t)) & 3u) << (2 * t);
-        } else {
-#pragma unroll
-          for (int t = 0; t < 8; t++)
-            if (t < nv) types |= (unsigned)(a.types[i0 + t] & 3u) << (2 * t);
-        }
+        types = load_type_octet(a.types, i0, nv);
       }
     }
     // deltas d = e0 + t use q[t + 1] - q[t]; q[8] is the next lane's q[0]

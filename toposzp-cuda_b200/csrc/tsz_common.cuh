@@ -97,15 +97,17 @@ __host__ __device__ __forceinline__ float code_float(uint32_t c) {
   return v;
 }
 
-// (int)((double)x * inv) with the device conversion (truncation, saturation)
+// (int)((double)x * inv): the C conversion of the reference's kernels
+// (truncation toward zero; on sm_100a values beyond the int range saturate and
+// NaN converts to INT_MIN)
 __device__ __forceinline__ int quantize(float x, double inv) {
-  return __double2int_rz(__dmul_rn((double)x, inv));
+  return (int)__dmul_rn((double)x, inv);
 }
 
 // quantization bin of a critical point: float add first, then the double multiply
 // (SZp/src/szp_cuda_topology.cu:67)
 __device__ __forceinline__ int quant_bin(float c, float eb, double inv) {
-  return __double2int_rz(__dmul_rn((double)__fadd_rn(c, eb), inv));
+  return (int)__dmul_rn((double)__fadd_rn(c, eb), inv);
 }
 
 // bit count of a block: floor(log2f((float)max)) + 1 (SZp/src/szp_cuda_topology.cu:558)

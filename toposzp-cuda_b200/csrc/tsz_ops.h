@@ -16,6 +16,18 @@ constexpr unsigned long long kMaxElements = 1ull << 40;
 // below kMaxElements without overflow) and fills the kernel geometry.
 bool geom_elements(const szp_b200_geom &g, unsigned long long *n, Geom *out);
 
+// Largest topology stream (header, blocks with tags, slack) of n elements.
+size_t topo_stream_bound(unsigned long long n, int B);
+
+// Block size inside the reference's range [1, 257]; sets the error otherwise.
+bool valid_block_size(int B, const char *fn);
+
+// Types (1..3) of a critical-point list into a zeroed byte-per-element array:
+// records of `stride` ints (x, y, type, ... in 2D; x, y, z, type, ... in 3D),
+// points outside the grid or with other types skipped.  Enqueued on s.
+cudaError_t launch_mark_types(const int *d_cps, int stride, long long count, const Geom &g, unsigned long long n,
+                              unsigned char *d_types, cudaStream_t s);
+
 // Runs one encoder pass on ctx->stream and waits for it.
 //   out: payload destination (stream base + 8); the 8-byte header is written here too.
 //   totals_out (host): payload bytes, cps, extrema.

@@ -207,3 +207,111 @@ def small_field(dims, seed=0, kind="bumps", noise=1e-3) -> np.ndarray:
     if kind == "band":
         return band_limited(dims, seed)
     raise ValueError(kind)
+
+
+# ---------------------------------------------------------------------------
+# float64 fields for the fp64 3D path
+# ---------------------------------------------------------------------------
+
+def f64_field(dims, seed=0, kind="smooth") -> np.ndarray:
+    """Seeded float64 3D fields (computed in double, never cast to float32).
+
+    smooth:  sum of 8 separable cosines (0.5..4 cycles per axis, random phase,
+             amplitude N(0, 1)) plus N(0, 1e-4) noise
+    noise:   N(0, 1) white noise (most interior points are critical and many
+             saddles lose their shape under quantization)
+    special: the smooth field with +-1e300, +-inf and NaN planted at seeded
+             positions and a band of values just inside / outside the int32
+             range of the quantizer (scaled by 1/eb = 1e3)
+    """
+    dims = tuple(int(d) for d in dims)
+    rng = np.random.default_rng(seed)
+    if kind == "noise":
+        return rng.standard_normal(dims)
+    out = np.zeros(dims, dtype=np.float64)
+    axes = [np.arange(s, dtype=np.float64) / max(s, 1) for s in dims]
+    for _ in range(8):
+        term = rng.standard_normal()
+        for a, ax in enumerate(axes):
+            f = rng.uniform(0.5, 4.0)
+            ph = rng.uniform(0.0, 2.0 * math.pi)
+            shape = [1] * len(dims)
+            shape[a] = dims[a]
+            term = term * np.cos(2.0 * math.pi * f * ax + ph).reshape(shape)
+        out += term
+    out += rng.normal(0.0, 1e-4, size=dims)
+    if kind == "special":
+        flat = out.reshape(-1)
+        pos = rng.choice(flat.size, size=min(flat.size, 64), replace=False)
+        vals = [1e300, -1e300, np.inf, -np.inf, np.nan,
+                2147483647.0 / 1e3, -2147483648.0 / 1e3, 2147483648.5 / 1e3, -2147483649.5 / 1e3]
+        for k, p in enumerate(pos):
+            flat[p] = vals[k % len(vals)]
+    elif kind != "smooth":
+        raise ValueError(kind)
+    return out
+
+
+def f64_critical_points(d: np.ndarray) -> np.ndarray:
+    """CriticalPoint3D records (x, y, z, type, 0, 0) of the strict 6-neighbour
+    classification of a float64 field, interior points only, raster order:
+    1 maximum, 2 minimum, 3 saddle (higher than both neighbours along one axis
+    and lower than both along another)."""
+    c = d[1:-1, 1:-1, 1:-1]
+    hi, lo = [], []
+    for a in range(3):
+        sl_m = [slice(1, -1)] * 3
+        sl_p = [slice(1, -1)] * 3
+        sl_m[a] = slice(0, -2)
+        sl_p[a] = slice(2, None)
+        m, p = d[tuple(sl_m)], d[tuple(sl_p)]
+        hi.append((c > m) & (c > p))
+        lo.append((c < m) & (c < p))
+    mx = hi[0] & hi[1] & hi[2]
+    mn = lo[0] & lo[1] & lo[2]
+    anyh = hi[0] | hi[1] | hi[2]
+    anyl = lo[0] | lo[1] | lo[2]
+    sd = anyh & anyl
+    t = np.zeros(c.shape, dtype=np.int32)
+    t[sd] = 3
+    t[mn] = 2
+    t[mx] = 1
+    x, y, z = np.nonzero(t)
+    rec = np.zeros((x.size, 6), dtype=np.int32)
+    rec[:, 0], rec[:, 1], rec[:, 2] = x + 1, y + 1, z + 1
+    rec[:, 3] = t[x, y, z]
+    return rec
+
+
+def f64_cases():
+    """The fp64 parity cases: name -> (dims, seed, kind, abs eb, blockSize,
+    extra records).  Extra records (x, y, z, type) are appended to the
+    classified list: points outside the grid, types outside 1..3 and saddles
+    on the boundary (tagged, never repaired)."""
+    edge = [(-1, 2, 2, 3), (2, 2, 99, 1), (0, 3, 3, 3), (3, 0, 4, 3), (4, 4, 0, 3), (5, 5, 5, 7), (6, 6, 6, 0)]
+    return {
+        "smooth_40x50x60": ((40, 50, 60), 11, "smooth", 1e-3, 64, []),
+        "noise_32x33x35": ((32, 33, 35), 12, "noise", 5e-2, 64, []),
+        "noise_tail_17x19x23_B7": ((17, 19, 23), 13, "noise", 2e-1, 7, edge),
+        "smooth_B257_24x30x41": ((24, 30, 41), 14, "smooth", 1e-4, 257, edge),
+        "special_20x21x22": ((20, 21, 22), 15, "special", 1e-3, 64, []),
+        "noise_B1_9x10x11": ((9, 10, 11), 16, "noise", 1e-1, 1, []),
+        "thin_3x40x50": ((3, 40, 50), 17, "noise", 1e-1, 32, []),
+        "smooth_128x128x128": ((128, 128, 128), 18, "smooth", 1e-5, 64, []),
+        "noise_96x96x96": ((96, 96, 96), 19, "noise", 5e-2, 64, []),
+    }
+
+
+def f64_case(name):
+    """(field, CriticalPoint3D records as int32 rows of 6, abs eb, blockSize)."""
+    dims, seed, kind, eb, B, extra = f64_cases()[name]
+    d = f64_field(dims, seed, kind)
+    cp = f64_critical_points(d)
+    if extra:
+        ex = np.zeros((len(extra), 6), dtype=np.int32)
+        ex[:, :4] = np.array(extra, dtype=np.int32)
+        # extra points replace none of the classified ones: skip duplicates
+        have = {tuple(r[:3]) for r in cp}
+        ex = np.array([r for r in ex if tuple(r[:3]) not in have], dtype=np.int32).reshape(-1, 6)
+        cp = np.concatenate([cp, ex])
+    return d, np.ascontiguousarray(cp, dtype=np.int32), eb, B

@@ -33,6 +33,7 @@ EXPORTS = [
     "szp_cuda_sort_critical_points_3d",
     "szp_cuda_compress_sort_positions_3d",
     "szp_cuda_float_compress_topology_3d",
+    "szp_cuda_double_compress_topology_3d",
     "szp_cuda_float_decompress_randomaccess_topology_preserved",
     "szp_cuda_decompress_sort_positions",
     "szp_b200_last_error",
@@ -50,6 +51,8 @@ EXPORTS = [
     "szp_b200_topo_decompress_host",
     "szp_b200_topo_encode_noalloc",
     "szp_b200_topo_check",
+    "szp_b200_double_compress_topology_3d_dev",
+    "szp_b200_f64_topo_scratch_bytes",
     "szp_b200_selftest_bounded_wait",
     "szp_b200_container_bound",
     "szp_b200_container_from_streams_dev",
@@ -156,6 +159,8 @@ def lib():
             "szp_cuda_float_compress_randomaccess_topology_preserved":
                 (vp, [vp, C.POINTER(sz), f, sz, i, vp, i, i, i]),
             "szp_cuda_float_compress_topology_3d": (vp, [vp, C.POINTER(sz), f, sz, i, vp, i, i, i, i]),
+            "szp_cuda_double_compress_topology_3d": (vp, [vp, C.POINTER(sz), C.c_double, sz, i, vp, i, i, i,
+                                                          i]),
             "szp_cuda_float_decompress_randomaccess_topology_preserved":
                 (None, [C.POINTER(vp), sz, f, i, vp, C.POINTER(vp)]),
             "szp_cuda_decompress_sort_positions": (vp, [vp, sz, i]),
@@ -175,6 +180,9 @@ def lib():
             "szp_b200_topo_encode_noalloc": (i, [vp, Geom, f, i, vp, sz, C.POINTER(sz), vp]),
             "szp_b200_topo_check": (i, [vp, vp, vp, Geom, f, C.POINTER(TopoReport)]),
             "szp_b200_selftest_bounded_wait": (i, [i, i, C.POINTER(i), C.POINTER(f)]),
+            "szp_b200_double_compress_topology_3d_dev": (i, [vp, vp, Geom, C.c_double, i, vp, sz, i, vp, sz,
+                                                             C.POINTER(sz), vp]),
+            "szp_b200_f64_topo_scratch_bytes": (sz, [sz, sz, i]),
             "szp_b200_container_bound": (sz, [sz, i, i]),
             "szp_b200_container_from_streams_dev": (i, [vp, vp, sz, vp, sz, Geom, i, sz, i, vp, sz,
                                                         C.POINTER(sz)]),
@@ -291,6 +299,21 @@ def compress_topology(data: np.ndarray, eb: float, block_size: int, cps: np.ndar
         ptr = lib().szp_cuda_float_compress_topology_3d(
             _p(d), C.byref(sz), eb, d.size, block_size, _p(cp) if len(cp) else None, len(cp),
             *d.shape)
+    if not ptr:
+        raise ToposzpError(last_error() or "compression returned NULL")
+    return _take(ptr, sz.value, np.uint8).tobytes()
+
+
+def double_compress_topology_3d(data: np.ndarray, eb: float, block_size: int, cps: np.ndarray) -> bytes:
+    """szp_cuda_double_compress_topology_3d: a 3D float64 field, the critical
+    points that mark its types (CP3_DT records), the topology stream."""
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    if d.ndim != 3:
+        raise ValueError("a 3D field is required")
+    cp = np.ascontiguousarray(cps)
+    sz = C.c_size_t(0)
+    ptr = lib().szp_cuda_double_compress_topology_3d(
+        _p(d), C.byref(sz), float(eb), d.size, block_size, _p(cp) if len(cp) else None, len(cp), *d.shape)
     if not ptr:
         raise ToposzpError(last_error() or "compression returned NULL")
     return _take(ptr, sz.value, np.uint8).tobytes()
@@ -475,6 +498,20 @@ class Context:
         if rc:
             raise ToposzpError(last_error())
         return rep.as_dict()
+
+    def compress_f64(self, d_data, shape, eb: float, block_size: int, d_cps, count: int, d_out,
+                     passes: int = 3, d_q=None) -> int:
+        """fp64 3D topology compression of device memory (d_cps: CriticalPoint3D
+        records on the device, or None); returns the stream length in d_out."""
+        out_len = C.c_size_t(0)
+        rc = lib().szp_b200_double_compress_topology_3d_dev(
+            self.ptr, C.c_void_p(d_data.data_ptr()), geom_of(shape), float(eb), block_size,
+            C.c_void_p(d_cps.data_ptr()) if d_cps is not None else None, count, passes,
+            C.c_void_p(d_out.data_ptr()), d_out.numel() * d_out.element_size(), C.byref(out_len),
+            C.c_void_p(d_q.data_ptr()) if d_q is not None else None)
+        if rc:
+            raise ToposzpError(last_error())
+        return out_len.value
 
     def postprocess(self, d_data, d_orig, d_types_int, d_sp, shape, eb: float, axis_stencil=False):
         rc = lib().szp_b200_topo_postprocess_dev(
