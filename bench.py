@@ -267,6 +267,54 @@ def reference_leg(f, planes, threads):
 
 
 # ---------------------------------------------------------------------------
+# reference GPU leg: the reference's own CUDA path on the same GPU and field
+# ---------------------------------------------------------------------------
+
+def reference_gpu_leg(T, f, eb, B, dims, topo, sort, sizes, ctx, reps=2):
+    """The reference's CUDA implementation (compiled from its sources into
+    oracle/_ref) run by its drivers' call sequence on the same field, timed by
+    wall clock per host-pointer call as its drivers do, in a child process;
+    with a bit-for-bit comparison of its outputs and this library's.  Its
+    post-processing is host code (the drivers') and is not part of these
+    times."""
+    import hashlib
+    import torch
+    import ref_cuda_run as R
+    if not R.available():
+        return None
+    n = f.n
+    r = R.run(f.data, eb, B, reps=reps, warmup=1)
+    tys = torch.empty(n, dtype=torch.uint8, device=topo.device)
+    raw = ctx.decompress(topo, sizes.topo_bytes, sort, sizes.sort_bytes, None, dims, eb, B, postprocess=0, types=tys)
+    sort_b = sort[: sizes.sort_bytes].cpu().numpy().tobytes()
+    sp = T.decompress_sort_positions(sort_b, sizes.extrema_count, B)
+
+    def sha(b):
+        return hashlib.sha256(b).hexdigest()
+    same = {"topo_stream": sha(topo[: sizes.topo_bytes].cpu().numpy().tobytes()) == r["topo"],
+            "raw_field": sha(raw.cpu().numpy().tobytes()) == r["raw"],
+            "types": sha(tys.cpu().numpy().tobytes()) == r["types"],
+            # the reference's CUDA sort writes dense rank - 1 for the first CP of
+            # each run of equal values (exclusive scan); its OpenMP sort, which
+            # this library follows, writes the dense rank
+            "sort_positions_equal_dense_rank_of_reference_cps":
+                sha(np.ascontiguousarray(sp, dtype=np.int32).tobytes()) == r["sp_dense_raster"],
+            "reference_cuda_sort_is_dense_rank_minus_run_start": r["cuda_sort_relation"],
+            "sort_positions_bitwise": sha(np.ascontiguousarray(sp, dtype=np.int32).tobytes()) == r["sp_raster"],
+            "cp_count": r["cp_count"] == sizes.cp_count}
+    ms = r["ms"]
+    return {"compress_ms": ms["compress"], "decompress_ms": ms["decompress"],
+            "round_trip_ms": ms["compress"] + ms["decompress"],
+            "value": 4.0 * n / ((ms["compress"] + ms["decompress"]) * 1e-3) / 1e9, "unit": UNIT,
+            "steps_ms": {k: v for k, v in ms.items() if k not in ("compress", "decompress")},
+            "identical_outputs": same, "reps": r["reps"],
+            "what": "the reference's CUDA path (find, sort, sort-position and topology streams; topology and "
+                    "sort-position decode) built from its sources for sm_100a, host-pointer calls timed by "
+                    "wall clock as its drivers do; its post-processing runs on the host in its drivers and "
+                    "is not included"}
+
+
+# ---------------------------------------------------------------------------
 # batched leg: 256 mixed fields (seed 3) in one batch vs back-to-back plain calls
 # ---------------------------------------------------------------------------
 
@@ -508,6 +556,8 @@ def parse():
     ap.add_argument("--cpu-planes", type=int, default=0,
                     help="planes in the CPU baseline sample (0: the whole field)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own CUDA path on the same field")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-e2e-pipelined", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain leg")
@@ -786,6 +836,10 @@ def main():
     if not args.no_serve:
         served = serve_leg(T, dev, nreq=args.serve_requests, slots=args.serve_slots)
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_leg(T, f, eb, B, dims, topo, sort, sizes, ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = reference_leg(f, args.cpu_planes or f.dims[0], os.cpu_count() or 1)
@@ -811,6 +865,7 @@ def main():
             "stages_ms": stages,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "e2e": e2e,
             "batched": batched,
             "served": served,

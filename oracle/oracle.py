@@ -15,8 +15,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libszp_ref.so")
-# the reference's CUDA 3D topology library (runs on a GPU; fixture generation only)
-REF_CUDA_SO = os.path.join(HERE, "_ref", "libszp_ref_cuda3d.so")
+# the reference's CUDA library for the path (runs on a GPU; fixtures and the
+# reference GPU timing only)
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libszp_ref_cuda.so")
 # reference source tree: the build argument, else $TOPOSZP_REF_SRC (no default:
 # without either, an already built _ref/libszp_ref.so is used as it is)
 REF_SRC = os.environ.get("TOPOSZP_REF_SRC")

@@ -1,11 +1,11 @@
-// Build-time shim (oracle/_ref only): the reference's CUDA 3D topology
-// library (CP finder, sort, sort-position compressor, fp32 and fp64
-// topology compressors) compiled from its source file where it lies.
+// Build-time shim (oracle/_ref only): one of the reference's CUDA source
+// files (REF_CUDA_SRC: the 2D and 3D topology libraries, the decompressors)
+// compiled where it lies.
 //
 // The library's common header does not compile under nvcc 12.9 (its
 // dimension check jumps with goto over an initialised declaration, which is
-// ill-formed C++), and the library uses five names from it.  The shim defines
-// the header's include guard and supplies those five with the header's
+// ill-formed C++), and these files use six names from it.  The shim defines
+// the header's include guard and supplies those six with the header's
 // contracts: on a CUDA error, a block size outside [1, max + 1], a dimension
 // <= 0 or a product of dimensions that overflows size_t, print a message and
 // exit the process.
@@ -16,6 +16,7 @@
 
 #define SZP_CUDA_COMMON_CUH 1
 #define SZP_CUDA_TOPO_MAX_BLOCK 256
+#define SZP_CUDA_MAX_BLOCK 1024
 
 #define CUDA_CHECK(call)                                                        \
   do {                                                                          \
@@ -44,4 +45,8 @@ static inline size_t szp_cuda_validate_dims(int d1, int d2, int d3, const char *
   return a * b * c;
 }
 
-#include REF_CUDA_3D
+static inline size_t szp_cuda_validate_dims_2d(int rows, int cols, const char *fn) {
+  return szp_cuda_validate_dims(rows, cols, 1, fn);
+}
+
+#include REF_CUDA_SRC

@@ -6,9 +6,9 @@ own CUDA 3D topology compressors on the fp64 parity cases
   f32  szp_cuda_float_compress_topology_3d(float32 cast of the field,
        float32 eb, blockSize, the same CP list)
 
-The reference library is oracle/_ref/libszp_ref_cuda3d.so, compiled from the
-reference's szp_cuda_topology_3d.cu by `make -C oracle refcuda REF=<tree>`;
-it runs on a GPU.  Each call runs in a child process (the reference exits the
+The reference library is oracle/_ref/libszp_ref_cuda.so, compiled from the
+reference's CUDA sources by `make -C oracle refcuda REF=<tree>`; it runs on a
+GPU.  Each call runs in a child process (the reference exits the
 process on a CUDA error).  The oracle's restatement of both compressors is
 checked against the reference's bytes on every case before anything is
 written.  Run from the repository root on a machine with a GPU:
