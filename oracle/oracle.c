@@ -637,6 +637,186 @@ int ora_decode_ints(const uint8_t *s, size_t len, size_t n, int B, int *out, siz
 }
 
 /* ------------------------------------------------------------------ */
+/* plain (non-topology) codec: random-access and threadblock modes,    */
+/* float and double (SZp/src/szp_cuda_compress.cu:122-360, 384-802;   */
+/* SZp/src/szp_cuda_decompress.cu:176-328, 480-665, 810-1070)          */
+/* ------------------------------------------------------------------ */
+
+static int quant_elem(const void *d, int dbl, size_t i, double inv)
+{
+    return dbl ? trunc_sat(((const double *)d)[i] * inv) : trunc_sat((double)((const float *)d)[i] * inv);
+}
+
+/* [bit count][sign bits][magnitudes] of the cnt deltas q[j+1] - q[j]; the
+ * bit-count byte is always written, the rest only when it is not 0
+ * (SZp/src/szp_cuda_compress.cu:296-357). */
+static size_t encode_deltas(const int *q, size_t cnt, uint8_t *o)
+{
+    uint8_t *p = o;
+    unsigned maxm = 0;
+    for (size_t j = 0; j < cnt; j++) {
+        unsigned ud = (unsigned)q[j + 1] - (unsigned)q[j];
+        unsigned m = (int)ud < 0 ? 0u - ud : ud;
+        if (m > maxm) maxm = m;
+    }
+    unsigned bc = ora_bitcount(maxm);
+    *p++ = (uint8_t)bc;
+    if (!bc) return 1;
+    size_t sb = (cnt + 7) / 8;
+    memset(p, 0, sb);
+    for (size_t j = 0; j < cnt; j++) {
+        unsigned ud = (unsigned)q[j + 1] - (unsigned)q[j];
+        if ((int)ud < 0) p[j / 8] |= (uint8_t)(1u << (7 - j % 8));
+    }
+    p += sb;
+    unsigned fb = bc / 8, rem = bc % 8;
+    for (size_t j = 0; j < cnt; j++) {
+        unsigned ud = (unsigned)q[j + 1] - (unsigned)q[j];
+        unsigned v = ((int)ud < 0 ? 0u - ud : ud) >> rem;
+        for (unsigned t = 0; t < fb; t++) { *p++ = (uint8_t)(v & 0xFF); v >>= 8; }
+    }
+    if (rem) {
+        size_t rb = (rem * cnt + 7) / 8;
+        memset(p, 0, rb);
+        for (size_t j = 0; j < cnt; j++) {
+            unsigned ud = (unsigned)q[j + 1] - (unsigned)q[j];
+            unsigned v = ((int)ud < 0 ? 0u - ud : ud) & ((1u << rem) - 1u);
+            for (unsigned b = 0; b < rem; b++) {
+                size_t bit = j * rem + b;
+                if ((v >> (rem - 1 - b)) & 1u) p[bit / 8] |= (uint8_t)(1u << (7 - bit % 8));
+            }
+        }
+        p += rb;
+    }
+    return (size_t)(p - o);
+}
+
+/* Compressed stream of the CUDA plain compressors: [T eb][u64 0][body]
+ * (T float or double; one chunk).  Random access (tb == 0): blocks of B
+ * elements, each [i32 anchor][bit count if the block has > 1 element][signs]
+ * [magnitudes] (:122-243, 384-474).  Threadblock (tb == 1): [i32 q0], then
+ * blocks of B deltas over elements 1 .. n-1, each [bit count][signs]
+ * [magnitudes], deltas chained across blocks (:245-357, 550-607).  q =
+ * (int)(x * (1/eb)) in double, inv = 1.0 / (double)eb.  eb carries the
+ * caller's float bound exactly when dbl == 0. */
+size_t ora_plain_compress(const void *d, int dbl, size_t n, double eb, int B, int tb, uint8_t *out)
+{
+    size_t es = dbl ? 8 : 4;
+    if (dbl) memcpy(out, &eb, 8);
+    else { float f = (float)eb; memcpy(out, &f, 4); }
+    memset(out + es, 0, 8);
+    size_t off = es + 8;
+    double inv = 1.0 / eb;
+    int *q = (int *)malloc(((size_t)B + 1) * sizeof(int));
+    if (!tb) {
+        for (size_t s = 0; s < n; s += (size_t)B) {
+            size_t m = (n - s < (size_t)B) ? n - s : (size_t)B;
+            for (size_t j = 0; j < m; j++) q[j] = quant_elem(d, dbl, s + j, inv);
+            off += encode_block(q, m, NULL, 0, out + off);
+        }
+    } else if (n) {
+        int prior = quant_elem(d, dbl, 0, inv);
+        memcpy(out + off, &prior, 4);
+        off += 4;
+        for (size_t i = 1; i < n; i += (size_t)B) {
+            size_t m = (n - i < (size_t)B) ? n - i : (size_t)B;
+            q[0] = prior;
+            for (size_t j = 0; j < m; j++) q[j + 1] = quant_elem(d, dbl, i + j, inv);
+            off += encode_deltas(q, m, out + off);
+            prior = q[m];
+        }
+    }
+    free(q);
+    return off;
+}
+
+size_t ora_plain_bound(size_t n, int B, int dbl)
+{
+    size_t nb = (n + B - 1) / B + 1;
+    return (dbl ? 8 : 4) + 8 + 4 + nb * ora_block_bytes((size_t)B + 1, 32, 0, 1) + 64;
+}
+
+static void store_deq(void *out, int dbl, size_t i, int q, double eb)
+{
+    if (dbl) ((double *)out)[i] = (double)q * eb;
+    else ((float *)out)[i] = (float)q * (float)eb;
+}
+
+/* Random-access decompression of s = the stream after its T eb header, as
+ * the reference API receives it: thread-count detection and walk as for the
+ * sort-position stream (:176-328), values (T)q * eb (:523-595). */
+int ora_plain_decompress_ra(const uint8_t *s, size_t len, size_t n, double eb, int B, int dbl, void *out,
+                            size_t *used)
+{
+    int *q = (int *)malloc((n ? n : 1) * sizeof(int));
+    int rc = ora_decode_ints(s, len, n, B, q, used);
+    if (!rc)
+        for (size_t i = 0; i < n; i++) store_deq(out, dbl, i, q[i], eb);
+    free(q);
+    return rc;
+}
+
+/* Threadblock decompression (:480-518, 597-665, 905-984).  Thread count:
+ * the largest t <= 256 whose first t offsets are non-decreasing and at most
+ * 4n + 4, stopping at the first t that is not (1 when the first offset is
+ * not 0); each chunk [lo, hi) of n / t elements is [i32 q0][blocks of B
+ * deltas].  A detected table whose chunks do not walk inside 4n + 4 bytes is
+ * read as one chunk (the reference decodes past its buffer there); -1 when
+ * that does not walk either. */
+int ora_plain_decompress_tb(const uint8_t *s, size_t len, size_t n, double eb, int B, int dbl, void *out,
+                            size_t *used)
+{
+    size_t maxc = 4 * n + 4, lim = len < maxc ? len : maxc;
+    unsigned T = 0;
+    for (unsigned t = 1; t <= 256; t++) {
+        if ((size_t)8 * t > len || rd_u64(s) != 0) break;
+        int ok = 1;
+        for (unsigned k = 1; k < t; k++) {
+            unsigned long long a = rd_u64(s + 8 * k), b = rd_u64(s + 8 * (k - 1));
+            if (a > maxc || a < b) { ok = 0; break; }
+        }
+        if (!ok) break;
+        if ((size_t)8 * t + 5 <= maxc) T = t;
+    }
+    if (T == 0) T = 1;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        size_t hdr = (size_t)8 * T, tbs = n / T, end = hdr;
+        int bad = 0;
+        for (unsigned c = 0; c < T && !bad; c++) {
+            size_t lo = c * tbs, hi = (c == T - 1) ? n : (c + 1) * tbs;
+            if (lo >= hi) continue;
+            size_t pos = hdr + (size_t)rd_u64(s + 8 * c);
+            if (pos + 4 > lim) { bad = 1; break; }
+            int prior = (int)rd_u32(s + pos);
+            pos += 4;
+            store_deq(out, dbl, lo, prior, eb);
+            for (size_t i = lo + 1; i < hi; i += (size_t)B) {
+                size_t m = (i + B > hi) ? hi - i : (size_t)B;
+                if (pos >= lim) { bad = 1; break; }
+                unsigned bc = s[pos++];
+                if (bc > 32) { bad = 1; break; }
+                const uint8_t *sg = s + pos, *mg = sg + (m + 7) / 8;
+                if (bc) pos += (m + 7) / 8 + magnitude_bytes(m, bc);
+                if (pos > lim) { bad = 1; break; }
+                for (size_t j = 0; j < m; j++) {
+                    if (bc) {
+                        unsigned v = extract_mag(mg, j, m, bc);
+                        int neg = (sg[j >> 3] >> (7 - (j & 7))) & 1;
+                        prior = (int)((unsigned)prior + (neg ? 0u - v : v));
+                    }
+                    store_deq(out, dbl, i + j, prior, eb);
+                }
+            }
+            if (pos > end) end = pos;
+        }
+        if (!bad) { if (used) *used = end; return 0; }
+        if (T == 1) return -1;
+        T = 1;
+    }
+    return -1;
+}
+
+/* ------------------------------------------------------------------ */
 /* 2D post-processing (example/test_cuda_topology.cu:117-326, :493-531) */
 /* ------------------------------------------------------------------ */
 

@@ -61,6 +61,12 @@ size_t ora_ints_bound(size_t n, int B);
 int ora_decode_topo(const uint8_t *s, size_t len, size_t n, float eb, int B,
                     float *out, int *fn, size_t *used);
 int ora_decode_ints(const uint8_t *s, size_t len, size_t n, int B, int *out, size_t *used);
+size_t ora_plain_compress(const void *d, int dbl, size_t n, double eb, int B, int tb, uint8_t *out);
+size_t ora_plain_bound(size_t n, int B, int dbl);
+int ora_plain_decompress_ra(const uint8_t *s, size_t len, size_t n, double eb, int B, int dbl, void *out,
+                            size_t *used);
+int ora_plain_decompress_tb(const uint8_t *s, size_t len, size_t n, double eb, int B, int dbl, void *out,
+                            size_t *used);
 
 /* post-processing (serial raster semantics of the reference CUDA drivers) */
 int ora_post_2d(float *data, const float *orig, const int *fn, const int *sp,
