@@ -117,6 +117,66 @@ SZP_B200_API void szp_cuda_float_decompress_randomaccess_topology_preserved(
 SZP_B200_API int *szp_cuda_decompress_sort_positions(
     unsigned char *cmpBytes, size_t critical_count, int blockSize);
 
+/* Plain (non-topology) codec.  Compressed stream: [T eb][u64 0][body], T the
+ * element type; the decompressors take the stream after its T header, as the
+ * reference's do.  blockSize 1..1025. */
+/* replaces SZp/include/szp_cuda_compress.cuh:22 (szp_cuda_compress.cu:718) */
+SZP_B200_API unsigned char *szp_cuda_float_compress_randomaccess(float *oriData, size_t *outSize,
+                                                                 float absErrBound, size_t nbEle, int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:26 */
+SZP_B200_API void szp_cuda_float_compress_randomaccess_arg(unsigned char *output, float *oriData, size_t *outSize,
+                                                           float absErrBound, size_t nbEle, int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:30 */
+SZP_B200_API unsigned char *szp_cuda_double_compress_randomaccess(double *oriData, size_t *outSize,
+                                                                  double absErrBound, size_t nbEle, int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:34 */
+SZP_B200_API void szp_cuda_double_compress_randomaccess_arg(unsigned char *output, double *oriData,
+                                                            size_t *outSize, double absErrBound, size_t nbEle,
+                                                            int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:40 */
+SZP_B200_API unsigned char *szp_cuda_float_compress_threadblock(float *oriData, size_t *outSize,
+                                                                float absErrBound, size_t nbEle, int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:44 */
+SZP_B200_API void szp_cuda_float_compress_threadblock_arg(unsigned char *output, float *oriData, size_t *outSize,
+                                                          float absErrBound, size_t nbEle, int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:48 */
+SZP_B200_API unsigned char *szp_cuda_double_compress_threadblock(double *oriData, size_t *outSize,
+                                                                 double absErrBound, size_t nbEle, int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:52 */
+SZP_B200_API void szp_cuda_double_compress_threadblock_arg(unsigned char *output, double *oriData,
+                                                           size_t *outSize, double absErrBound, size_t nbEle,
+                                                           int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:58: q[0], q[i] - q[i-1] (malloc'd) */
+SZP_B200_API int *szp_cuda_float_direct_predict_quantization(float *oriData, size_t *outSize, float absErrBound,
+                                                             size_t nbEle, int blockSize);
+/* replaces SZp/include/szp_cuda_compress.cuh:62 (the same result) */
+SZP_B200_API int *szp_cuda_float_threadblock_predict_quantization(float *oriData, size_t *outSize,
+                                                                  float absErrBound, size_t nbEle, int blockSize);
+/* replaces SZp/include/szp_cuda_decompress.cuh:23 (szp_cuda_decompress.cu:990) */
+SZP_B200_API float *szp_cuda_float_decompress_randomaccess(size_t nbEle, float absErrBound, int blockSize,
+                                                           unsigned char *cmpBytes);
+/* replaces SZp/include/szp_cuda_decompress.cuh:27 */
+SZP_B200_API void szp_cuda_float_decompress_randomaccess_arg(float *newData, size_t nbEle, float absErrBound,
+                                                             int blockSize, unsigned char *cmpBytes);
+/* replaces SZp/include/szp_cuda_decompress.cuh:31 */
+SZP_B200_API double *szp_cuda_double_decompress_randomaccess(size_t nbEle, double absErrBound, int blockSize,
+                                                             unsigned char *cmpBytes);
+/* replaces SZp/include/szp_cuda_decompress.cuh:35 */
+SZP_B200_API void szp_cuda_double_decompress_randomaccess_arg(double *newData, size_t nbEle, double absErrBound,
+                                                              int blockSize, unsigned char *cmpBytes);
+/* replaces SZp/include/szp_cuda_decompress.cuh:43 */
+SZP_B200_API float *szp_cuda_float_decompress_threadblock(size_t nbEle, float absErrBound, int blockSize,
+                                                          unsigned char *cmpBytes);
+/* replaces SZp/include/szp_cuda_decompress.cuh:47 */
+SZP_B200_API void szp_cuda_float_decompress_threadblock_arg(float *newData, size_t nbEle, float absErrBound,
+                                                            int blockSize, unsigned char *cmpBytes);
+/* replaces SZp/include/szp_cuda_decompress.cuh:51 */
+SZP_B200_API double *szp_cuda_double_decompress_threadblock(size_t nbEle, double absErrBound, int blockSize,
+                                                            unsigned char *cmpBytes);
+/* replaces SZp/include/szp_cuda_decompress.cuh:55 */
+SZP_B200_API void szp_cuda_double_decompress_threadblock_arg(double *newData, size_t nbEle, double absErrBound,
+                                                             int blockSize, unsigned char *cmpBytes);
+
 /* ------------------------------------------------------------------ */
 /* Part 2: additions (no reference counterpart)                        */
 /* ------------------------------------------------------------------ */
@@ -292,6 +352,19 @@ SZP_B200_API int szp_b200_double_compress_topology_3d_dev(szp_b200_ctx *ctx, con
                                                           size_t *out_len, int *d_q);
 /* Device scratch the call above takes from the workspace. */
 SZP_B200_API size_t szp_b200_f64_topo_scratch_bytes(size_t n, size_t critical_count, int blockSize);
+
+/* Plain codec on device memory.  Bound of the whole stream ([T eb][u64 0]
+ * [body]; is_double selects T), compression of n elements into d_out (random
+ * access, or threadblock when threadblock != 0), and random-access
+ * decompression of a single-chunk stream (d_in: the stream after its T header,
+ * in_len bytes; block offsets parsed on the device).  Return 0 / -1. */
+SZP_B200_API size_t szp_b200_plain_bound(size_t n, int blockSize, int is_double, int threadblock);
+SZP_B200_API int szp_b200_plain_compress_dev(szp_b200_ctx *ctx, const void *d_data, int is_double, size_t n,
+                                             double absErrBound, int blockSize, int threadblock,
+                                             unsigned char *d_out, size_t out_cap, size_t *out_len);
+SZP_B200_API int szp_b200_plain_decompress_dev(szp_b200_ctx *ctx, const unsigned char *d_in, size_t in_len,
+                                               int is_double, size_t n, double absErrBound, int blockSize,
+                                               void *d_out);
 
 /* Bounded-wait self-test (no reference counterpart).  Every device wait of
  * the library gives up after a poll limit and reports an error instead of

@@ -782,6 +782,9 @@ int ora_plain_decompress_tb(const uint8_t *s, size_t len, size_t n, double eb, i
     for (int attempt = 0; attempt < 2; attempt++) {
         size_t hdr = (size_t)8 * T, tbs = n / T, end = hdr;
         int bad = 0;
+        /* a multi-chunk table must walk inside 4n + 4 bytes; one chunk is
+         * walked as far as the buffer goes, as the reference walks it */
+        lim = T > 1 ? (len < maxc ? len : maxc) : len;
         for (unsigned c = 0; c < T && !bad; c++) {
             size_t lo = c * tbs, hi = (c == T - 1) ? n : (c + 1) * tbs;
             if (lo >= hi) continue;

@@ -81,6 +81,10 @@ def lib():
             "ora_encode_topo": (sz, [vp, sz, f, i, vp, i, vp]),
             "ora_encode_ints": (sz, [vp, sz, i, i, vp]),
             "ora_double_compress_topo_3d": (sz, [vp, sz, d, i, vp, i, i, i, i, vp, vp]),
+            "ora_plain_compress": (sz, [vp, i, sz, d, i, i, vp]),
+            "ora_plain_bound": (sz, [sz, i, i]),
+            "ora_plain_decompress_ra": (i, [vp, sz, sz, d, i, i, vp, C.POINTER(sz)]),
+            "ora_plain_decompress_tb": (i, [vp, sz, sz, d, i, i, vp, C.POINTER(sz)]),
             "ora_topo_bound": (sz, [sz, i]),
             "ora_ints_bound": (sz, [sz, i]),
             "ora_decode_topo": (i, [vp, sz, sz, f, i, vp, vp, C.POINTER(sz)]),
@@ -242,6 +246,37 @@ def double_compress_topo_3d(data: np.ndarray, eb: float, B: int, types, dims, pa
     m = lib().ora_double_compress_topo_3d(_p(d), n, float(eb), B, _p(t), dims[0], dims[1], dims[2],
                                           passes, _p(q), _p(out))
     return (out[:m].tobytes(), q) if with_q else out[:m].tobytes()
+
+
+def plain_compress(data: np.ndarray, eb: float, B: int, threadblock: bool = False) -> bytes:
+    """Plain-codec stream [T eb][u64 0][body] of the CUDA compressors (T: the
+    dtype of data, float32 or float64).  eb is the caller's bound (a float32
+    value for float32 data)."""
+    dbl = np.asarray(data).dtype == np.float64
+    d = np.ascontiguousarray(data, dtype=np.float64 if dbl else np.float32).reshape(-1)
+    ebv = float(eb) if dbl else float(np.float32(eb))
+    out = np.zeros(lib().ora_plain_bound(d.size, B, int(dbl)), dtype=np.uint8)
+    m = lib().ora_plain_compress(_p(d), int(dbl), d.size, ebv, B, int(threadblock), _p(out))
+    return out[:m].tobytes()
+
+
+def plain_decompress(stream: bytes, n: int, eb: float, B: int, dtype=np.float32, threadblock: bool = False,
+                     pad: int = 4096):
+    """Values of a plain stream (the compressor's whole output; decoded from
+    after its T header, as the reference's callers pass it)."""
+    dbl = np.dtype(dtype) == np.float64
+    es = 8 if dbl else 4
+    body = np.frombuffer(stream, dtype=np.uint8)[es:]
+    buf = np.zeros(body.size + pad, dtype=np.uint8)
+    buf[: body.size] = body
+    out = np.zeros(max(1, n), dtype=np.float64 if dbl else np.float32)
+    used = C.c_size_t(0)
+    fn = lib().ora_plain_decompress_tb if threadblock else lib().ora_plain_decompress_ra
+    ebv = float(eb) if dbl else float(np.float32(eb))
+    rc = fn(_p(buf), buf.size, n, ebv, B, int(dbl), _p(out), C.byref(used))
+    if rc:
+        raise ValueError("malformed plain stream")
+    return out[:n], used.value
 
 
 def encode_ints(v: np.ndarray, B: int, cpu_layout=False) -> bytes:

@@ -1,6 +1,6 @@
 // Build-time shim (oracle/_ref only): one of the reference's CUDA source
-// files (REF_CUDA_SRC: the 2D and 3D topology libraries, the decompressors)
-// compiled where it lies.
+// files (REF_CUDA_SRC: the 2D and 3D topology libraries, the decompressors,
+// the plain compressors) compiled where it lies.
 //
 // The library's common header does not compile under nvcc 12.9 (its
 // dimension check jumps with goto over an initialised declaration, which is

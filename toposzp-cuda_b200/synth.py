@@ -315,3 +315,68 @@ def f64_case(name):
         ex = np.array([r for r in ex if tuple(r[:3]) not in have], dtype=np.int32).reshape(-1, 6)
         cp = np.concatenate([cp, ex])
     return d, np.ascontiguousarray(cp, dtype=np.int32), eb, B
+
+
+# ---------------------------------------------------------------------------
+# 1-D inputs for the plain (non-topology) codec
+# ---------------------------------------------------------------------------
+
+def plain_field(n, seed=0, kind="wave", dtype=np.float32) -> np.ndarray:
+    """Seeded 1-D inputs: wave (two sines of incommensurate periods, amplitude
+    80), walk (a Gaussian random walk, step 0.3), uniform (U(-100, 100)),
+    steps (constant runs of random length and level, then a ramp), special
+    (the wave with +-inf, NaN, +-1e30 and values around the int32 range of
+    the quantizer at 1/eb = 1e3 planted at seeded positions)."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n, dtype=np.float64)
+    if kind in ("wave", "special"):
+        x = 80.0 * np.sin(i * 0.0123 + 0.4) + 20.0 * np.sin(i * 0.00071 + 1.3)
+    elif kind == "walk":
+        x = np.cumsum(rng.normal(0.0, 0.3, size=n))
+    elif kind == "uniform":
+        x = rng.uniform(-100.0, 100.0, size=n)
+    elif kind == "steps":
+        x = np.zeros(n)
+        p = 0
+        while p < n:
+            r = int(rng.integers(1, 200))
+            x[p:p + r] = rng.uniform(-50, 50)
+            p += r
+        x[n // 2:] += np.linspace(0.0, 10.0, n - n // 2)
+    else:
+        raise ValueError(kind)
+    if kind == "special" and n > 16:
+        pos = rng.choice(n, size=min(n, 32), replace=False)
+        vals = [np.inf, -np.inf, np.nan, 1e30, -1e30, 2147483.0, -2147483.5, 2147484.0, -2147485.0]
+        for k, p in enumerate(pos):
+            x[p] = vals[k % len(vals)]
+    return x.astype(dtype)
+
+
+def plain_cases():
+    """name -> (n, seed, kind, dtype, abs eb, blockSize, threadblock)."""
+    cases = {}
+    for dt in ("f32", "f64"):
+        for tb in (0, 1):
+            m = "tb" if tb else "ra"
+            base = [
+                ("wave_100k_B64", 100000, 21, "wave", 1e-3, 64),
+                ("walk_65537_B64", 65537, 22, "walk", 1e-2, 64),
+                ("uniform_3000_B7", 3000, 23, "uniform", 1e-4, 7),
+                ("steps_20000_B1025", 20000, 24, "steps", 1e-3, 1025),
+                ("special_5000_B64", 5000, 25, "special", 1e-3, 64),
+                ("walk_2051_B1", 2051, 26, "walk", 1e-1, 1),
+                ("wave_1_B64", 1, 27, "wave", 1e-3, 64),
+                ("wave_2_B64", 2, 28, "wave", 1e-3, 64),
+                ("walk_257_B256", 257, 29, "walk", 1e-3, 256),
+            ]
+            for name, n, seed, kind, eb, B in base:
+                cases["%s_%s_%s" % (dt, m, name)] = (n, seed, kind, dt, eb, B, tb)
+    return cases
+
+
+def plain_case(name):
+    """(field, abs eb, blockSize, threadblock)."""
+    n, seed, kind, dt, eb, B, tb = plain_cases()[name]
+    x = plain_field(n, seed, kind, np.float64 if dt == "f64" else np.float32)
+    return x, eb, B, bool(tb)

@@ -53,6 +53,27 @@ EXPORTS = [
     "szp_b200_topo_check",
     "szp_b200_double_compress_topology_3d_dev",
     "szp_b200_f64_topo_scratch_bytes",
+    "szp_cuda_float_compress_randomaccess",
+    "szp_cuda_float_compress_randomaccess_arg",
+    "szp_cuda_double_compress_randomaccess",
+    "szp_cuda_double_compress_randomaccess_arg",
+    "szp_cuda_float_compress_threadblock",
+    "szp_cuda_float_compress_threadblock_arg",
+    "szp_cuda_double_compress_threadblock",
+    "szp_cuda_double_compress_threadblock_arg",
+    "szp_cuda_float_direct_predict_quantization",
+    "szp_cuda_float_threadblock_predict_quantization",
+    "szp_cuda_float_decompress_randomaccess",
+    "szp_cuda_float_decompress_randomaccess_arg",
+    "szp_cuda_double_decompress_randomaccess",
+    "szp_cuda_double_decompress_randomaccess_arg",
+    "szp_cuda_float_decompress_threadblock",
+    "szp_cuda_float_decompress_threadblock_arg",
+    "szp_cuda_double_decompress_threadblock",
+    "szp_cuda_double_decompress_threadblock_arg",
+    "szp_b200_plain_bound",
+    "szp_b200_plain_compress_dev",
+    "szp_b200_plain_decompress_dev",
     "szp_b200_selftest_bounded_wait",
     "szp_b200_container_bound",
     "szp_b200_container_from_streams_dev",
@@ -183,6 +204,27 @@ def lib():
             "szp_b200_double_compress_topology_3d_dev": (i, [vp, vp, Geom, C.c_double, i, vp, sz, i, vp, sz,
                                                              C.POINTER(sz), vp]),
             "szp_b200_f64_topo_scratch_bytes": (sz, [sz, sz, i]),
+            "szp_cuda_float_compress_randomaccess": (vp, [vp, C.POINTER(sz), f, sz, i]),
+            "szp_cuda_float_compress_randomaccess_arg": (None, [vp, vp, C.POINTER(sz), f, sz, i]),
+            "szp_cuda_double_compress_randomaccess": (vp, [vp, C.POINTER(sz), C.c_double, sz, i]),
+            "szp_cuda_double_compress_randomaccess_arg": (None, [vp, vp, C.POINTER(sz), C.c_double, sz, i]),
+            "szp_cuda_float_compress_threadblock": (vp, [vp, C.POINTER(sz), f, sz, i]),
+            "szp_cuda_float_compress_threadblock_arg": (None, [vp, vp, C.POINTER(sz), f, sz, i]),
+            "szp_cuda_double_compress_threadblock": (vp, [vp, C.POINTER(sz), C.c_double, sz, i]),
+            "szp_cuda_double_compress_threadblock_arg": (None, [vp, vp, C.POINTER(sz), C.c_double, sz, i]),
+            "szp_cuda_float_direct_predict_quantization": (vp, [vp, C.POINTER(sz), f, sz, i]),
+            "szp_cuda_float_threadblock_predict_quantization": (vp, [vp, C.POINTER(sz), f, sz, i]),
+            "szp_cuda_float_decompress_randomaccess": (vp, [sz, f, i, vp]),
+            "szp_cuda_float_decompress_randomaccess_arg": (None, [vp, sz, f, i, vp]),
+            "szp_cuda_double_decompress_randomaccess": (vp, [sz, C.c_double, i, vp]),
+            "szp_cuda_double_decompress_randomaccess_arg": (None, [vp, sz, C.c_double, i, vp]),
+            "szp_cuda_float_decompress_threadblock": (vp, [sz, f, i, vp]),
+            "szp_cuda_float_decompress_threadblock_arg": (None, [vp, sz, f, i, vp]),
+            "szp_cuda_double_decompress_threadblock": (vp, [sz, C.c_double, i, vp]),
+            "szp_cuda_double_decompress_threadblock_arg": (None, [vp, sz, C.c_double, i, vp]),
+            "szp_b200_plain_bound": (sz, [sz, i, i, i]),
+            "szp_b200_plain_compress_dev": (i, [vp, vp, i, sz, C.c_double, i, i, vp, sz, C.POINTER(sz)]),
+            "szp_b200_plain_decompress_dev": (i, [vp, vp, sz, i, sz, C.c_double, i, vp]),
             "szp_b200_container_bound": (sz, [sz, i, i]),
             "szp_b200_container_from_streams_dev": (i, [vp, vp, sz, vp, sz, Geom, i, sz, i, vp, sz,
                                                         C.POINTER(sz)]),
@@ -317,6 +359,47 @@ def double_compress_topology_3d(data: np.ndarray, eb: float, block_size: int, cp
     if not ptr:
         raise ToposzpError(last_error() or "compression returned NULL")
     return _take(ptr, sz.value, np.uint8).tobytes()
+
+
+def plain_compress(data: np.ndarray, eb: float, block_size: int, threadblock: bool = False) -> bytes:
+    """szp_cuda_{float,double}_compress_{randomaccess,threadblock}: the whole
+    stream [T eb][u64 0][body] (T the dtype of data)."""
+    dbl = np.asarray(data).dtype == np.float64
+    d = np.ascontiguousarray(data, dtype=np.float64 if dbl else np.float32).reshape(-1)
+    kind = ("double" if dbl else "float") + ("_compress_threadblock" if threadblock else "_compress_randomaccess")
+    sz = C.c_size_t(0)
+    ptr = getattr(lib(), "szp_cuda_" + kind)(_p(d), C.byref(sz), float(eb), d.size, block_size)
+    if not ptr:
+        raise ToposzpError(last_error() or "compression returned NULL")
+    return _take(ptr, sz.value, np.uint8).tobytes()
+
+
+def plain_decompress(stream: bytes, n: int, eb: float, block_size: int, dtype=np.float32,
+                     threadblock: bool = False) -> np.ndarray:
+    """szp_cuda_{float,double}_decompress_*: stream is the compressor's whole
+    output; the entry point receives it after its T header, as the
+    reference's callers pass it."""
+    dbl = np.dtype(dtype) == np.float64
+    es = 8 if dbl else 4
+    s = np.frombuffer(stream, dtype=np.uint8)[es:].copy()
+    out = np.zeros(n, dtype=np.float64 if dbl else np.float32)
+    kind = ("double" if dbl else "float") + ("_decompress_threadblock_arg" if threadblock
+                                             else "_decompress_randomaccess_arg")
+    getattr(lib(), "szp_cuda_" + kind)(_p(out), n, float(eb), block_size, _p(s))
+    err = last_error()
+    if err:
+        raise ToposzpError(err)
+    return out
+
+
+def predict_quantization(data: np.ndarray, eb: float, threadblock: bool = False) -> np.ndarray:
+    d = _f32(data).reshape(-1)
+    name = "szp_cuda_float_threadblock_predict_quantization" if threadblock else \
+        "szp_cuda_float_direct_predict_quantization"
+    ptr = getattr(lib(), name)(_p(d), None, float(eb), d.size, 64)
+    if not ptr:
+        raise ToposzpError(last_error() or "quantization returned NULL")
+    return _take(ptr, 4 * d.size, np.int32)
 
 
 def decompress_topology(stream: bytes, n: int, eb: float, block_size: int):
@@ -512,6 +595,30 @@ class Context:
         if rc:
             raise ToposzpError(last_error())
         return out_len.value
+
+    def plain_compress(self, d_data, eb: float, block_size: int, d_out, threadblock: bool = False) -> int:
+        """Plain-codec stream of a device tensor (float32 or float64) into d_out
+        (uint8 device tensor); returns its length."""
+        import torch
+        dbl = d_data.dtype == torch.float64
+        out_len = C.c_size_t(0)
+        rc = lib().szp_b200_plain_compress_dev(self.ptr, C.c_void_p(d_data.data_ptr()), int(dbl), d_data.numel(),
+                                               float(eb), block_size, int(threadblock), C.c_void_p(d_out.data_ptr()),
+                                               d_out.numel(), C.byref(out_len))
+        if rc:
+            raise ToposzpError(last_error())
+        return out_len.value
+
+    def plain_decompress(self, d_stream, length: int, n: int, eb: float, block_size: int, d_out) -> None:
+        """Random-access decode of a device stream written by plain_compress
+        (the whole stream, T header included) into d_out."""
+        import torch
+        dbl = d_out.dtype == torch.float64
+        es = 8 if dbl else 4
+        rc = lib().szp_b200_plain_decompress_dev(self.ptr, C.c_void_p(d_stream.data_ptr() + es), length - es,
+                                                 int(dbl), n, float(eb), block_size, C.c_void_p(d_out.data_ptr()))
+        if rc:
+            raise ToposzpError(last_error())
 
     def postprocess(self, d_data, d_orig, d_types_int, d_sp, shape, eb: float, axis_stencil=False):
         rc = lib().szp_b200_topo_postprocess_dev(
