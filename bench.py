@@ -266,6 +266,181 @@ def reference_leg(f, planes, threads):
                       % (what, sample.size, t)}
 
 
+def cpu_reference_run_2d(field: np.ndarray, eb: float, B: int, threads: int):
+    """One round trip of the reference's own CPU path on a 2D field, with the
+    CPU decompress driver's own post-processing (its a15 variant): find ->
+    sort -> sort-position stream -> topology stream -> decompress ->
+    sort-position decode -> locks, false-negative saddles, adaptive RBF,
+    stencils, extremum restoration.  Returns (compress s, decompress s)."""
+    import oracle as O
+    O.set_ref_threads(threads)
+    d = np.ascontiguousarray(field, dtype=np.float32)
+    t0 = time.perf_counter()
+    cp = O.ref_sort_cp(O.ref_find_cp(d, eb), d)
+    O.set_ref_threads(1)   # the sort-position compressor's use after free (see cpu_reference_run)
+    sp_stream = O.ref_compress_sp(cp, B)
+    O.set_ref_threads(threads)
+    topo = O.ref_compress_topo(d, eb, B, cp)
+    t1 = time.perf_counter()
+    raw, fn = O.ref_decompress_topo(topo, d.size, eb, B)
+    e = int(np.count_nonzero((cp["type"] == 1) | (cp["type"] == 2)))
+    sp = O.ref_decompress_sp(sp_stream[8:], e, B) if e else None
+    O.ref_post_cpu2d(raw.reshape(d.shape), fn.reshape(d.shape), sp, eb)
+    return t1 - t0, time.perf_counter() - t1
+
+
+def c1_leg(T, dev, steps, threads, rank0):
+    """C1, the 2D 1800x3600 bump field (abs eb 1e-3, blockSize 64): this
+    library's fused round trip on the device (each step timed by CUDA events
+    on the library's stream, L2 flushed between steps: the field, 26 MB, fits
+    in L2) and through the host-buffer C ABI, and the reference's CPU path with
+    its CPU driver's post-processing at all host threads and at one thread."""
+    import ctypes as C
+    import torch
+    f = synth.config1()
+    eb, B, dims, n = f.abs_eb(), f.block_size, f.dims, f.n
+    stream = torch.cuda.Stream(device=dev)
+    ctx = T.Context(stream.cuda_stream)
+    L = T.lib()
+    d = torch.from_numpy(f.data.reshape(-1)).to(dev)
+    topo = torch.empty(L.szp_b200_topo_bound(n, B), dtype=torch.uint8, device=dev)
+    sort = torch.empty(L.szp_b200_sort_bound(n, B), dtype=torch.uint8, device=dev)
+    idx = torch.empty(2 * ((n + B - 1) // B), dtype=torch.int64, device=dev)
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    flush = torch.empty(64 << 22, dtype=torch.float32, device=dev)   # 256 MiB > L2
+    sizes = T.Sizes()
+
+    def step():
+        if L.szp_b200_topo_compress_dev(ctx.ptr, C.c_void_p(d.data_ptr()), T.geom_of(dims), eb, B,
+                                        C.c_void_p(topo.data_ptr()), C.c_void_p(sort.data_ptr()),
+                                        C.c_void_p(idx.data_ptr()), C.byref(sizes)):
+            raise T.ToposzpError(T.last_error())
+        if L.szp_b200_topo_decompress_dev(ctx.ptr, C.c_void_p(topo.data_ptr()), sizes.topo_bytes,
+                                          C.c_void_p(sort.data_ptr()), sizes.sort_bytes,
+                                          C.c_void_p(idx.data_ptr()), T.geom_of(dims), eb, B,
+                                          C.c_void_p(out.data_ptr()), None, 1):
+            raise T.ToposzpError(T.last_error())
+
+    for _ in range(3):
+        step()
+    tot = 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    ms = tot / steps
+    rep = ctx.topo_check(d, out, dims, eb)
+    # end to end through the host-buffer calls (pinned buffers)
+    h_f = torch.from_numpy(f.data.reshape(dims)).pin_memory().numpy()
+    h_t = torch.empty(L.szp_b200_topo_bound(n, B), dtype=torch.uint8).pin_memory().numpy()
+    h_s = torch.empty(L.szp_b200_sort_bound(n, B), dtype=torch.uint8).pin_memory().numpy()
+    h_o = torch.empty(dims, dtype=torch.float32).pin_memory().numpy()
+    for _ in range(2):
+        sz = ctx.compress_host(h_f, eb, B, h_t, h_s)
+        ctx.decompress_host(h_t, sz.topo_bytes, h_s, sz.sort_bytes, dims, eb, B, h_o, 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sz = ctx.compress_host(h_f, eb, B, h_t, h_s)
+        ctx.decompress_host(h_t, sz.topo_bytes, h_s, sz.sort_bytes, dims, eb, B, h_o, 1)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / steps
+    res = {"workload": "c1: 2D %dx%d fp32 bump field, abs eb %g, blockSize %d, fused compress + decompress + "
+                       "post-processing" % (dims[0], dims[1], eb, B),
+           "value": 4.0 * n / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
+           "l2": "flushed between steps (256 MiB write outside the timed region)",
+           "e2e": {"value": 4.0 * n / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
+                   "timing": "wall clock around the host-buffer calls"},
+           "cps": sizes.cp_count, "extrema": sizes.extrema_count,
+           "topology": {"preserved": rep["preserved"], "orig_cps": rep["orig_cps"][0],
+                        "max_err_over_eb": rep["max_err"] / eb, "over_2eb": rep["over_2eb"]}}
+    ctx.close()
+    if rank0:
+        import oracle as O
+        if O.ref_available() and O.ref_cpu2d_available():
+            cpu = {}
+            for th, key in ((threads, "all_threads"), (1, "one_thread")):
+                tc, td = cpu_reference_run_2d(f.data, eb, B, th)
+                cpu[key] = {"threads": th, "compress_s": tc, "decompress_s": td,
+                            "value": 4.0 * n / (tc + td) / 1e9, "unit": UNIT}
+            cpu["what"] = ("the reference's OpenMP library (find, sort, both streams, decode) and its CPU "
+                           "decompress driver's own post-processing, whole C1 field")
+            cpu["cpu"] = cpu_model()
+            res["cpu_reference"] = cpu
+    return res
+
+
+def plain_leg(T, dev, f, steps, rank0):
+    """The plain (non-topology) codec, random-access mode, on the 512^3 field:
+    device compress + decompress through the device entry points (CUDA events
+    on the library's stream, input larger than L2), the same through the
+    reference-compatible host entry points, and the reference's own CUDA codec
+    on the same field (host-pointer calls, wall clock), with the streams
+    compared byte for byte."""
+    import hashlib
+    import torch
+    eb, B, n = f.abs_eb(), f.block_size, f.n
+    stream = torch.cuda.Stream(device=dev)
+    ctx = T.Context(stream.cuda_stream)
+    L = T.lib()
+    x = torch.from_numpy(f.data.reshape(-1)).to(dev)
+    buf = torch.empty(L.szp_b200_plain_bound(n, B, 0, 0), dtype=torch.uint8, device=dev)
+    y = torch.empty_like(x)
+    m = 0
+    for _ in range(2):
+        m = ctx.plain_compress(x, eb, B, buf)
+        ctx.plain_decompress(buf, m, n, eb, B, y)
+    tc = td = 0.0
+    for _ in range(steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        m = ctx.plain_compress(x, eb, B, buf)
+        e[1].record(stream)
+        ctx.plain_decompress(buf, m, n, eb, B, y)
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        tc += e[0].elapsed_time(e[1])
+        td += e[1].elapsed_time(e[2])
+    tc /= steps
+    td /= steps
+    stream_bytes = m
+    ours_sha = hashlib.sha256(buf[:m].cpu().numpy().tobytes()).hexdigest()
+    ctx.close()
+    peak, _ = peaks()
+    ac = (4.0 * n + stream_bytes) / (tc * 1e-3) / 1e9
+    ad = (4.0 * n + stream_bytes) / (td * 1e-3) / 1e9
+    res = {"workload": "plain codec, random access, float: the %s field, abs eb %g, blockSize %d" % (f.name, eb, B),
+           "compress_ms": tc, "decompress_ms": td,
+           "value": 4.0 * n / ((tc + td) * 1e-3) / 1e9, "unit": UNIT, "stream_bytes": stream_bytes,
+           "roofline": {"compress_gbs": ac, "compress_frac": ac / peak, "decompress_gbs": ad,
+                        "decompress_frac": ad / peak, "algorithmic_bytes": 4.0 * n + stream_bytes}}
+    # host entry points (the reference's signatures), wall clock
+    h = f.data.reshape(-1)
+    t0 = time.perf_counter()
+    s = T.plain_compress(h, eb, B)
+    t1 = time.perf_counter()
+    v = T.plain_decompress(s, n, eb, B)
+    t2 = time.perf_counter()
+    res["host_api"] = {"compress_ms": (t1 - t0) * 1e3, "decompress_ms": (t2 - t1) * 1e3,
+                       "value": 4.0 * n / (t2 - t0) / 1e9, "unit": UNIT,
+                       "max_err_over_eb": float(np.abs(v - h).max() / eb)}
+    if rank0:
+        import ref_cuda_run as R
+        if R.available():
+            r = R.run_plain(h, eb, B, reps=2, warmup=1)
+            res["reference_gpu"] = {"compress_ms": r["ms"]["compress"], "decompress_ms": r["ms"]["decompress"],
+                                    "value": 4.0 * n / ((r["ms"]["compress"] + r["ms"]["decompress"]) * 1e-3) / 1e9,
+                                    "unit": UNIT, "identical_stream": r["stream"] == hashlib.sha256(s).hexdigest()
+                                    and ours_sha == r["stream"],
+                                    "what": "the reference's CUDA plain codec, host-pointer calls, wall clock"}
+    return res
+
+
 # ---------------------------------------------------------------------------
 # reference GPU leg: the reference's own CUDA path on the same GPU and field
 # ---------------------------------------------------------------------------
@@ -556,6 +731,8 @@ def parse():
     ap.add_argument("--cpu-planes", type=int, default=0,
                     help="planes in the CPU baseline sample (0: the whole field)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-c1", action="store_true", help="skip the 2D 1800x3600 leg")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-codec leg")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA path on the same field")
     ap.add_argument("--no-e2e", action="store_true")
@@ -836,6 +1013,14 @@ def main():
     if not args.no_serve:
         served = serve_leg(T, dev, nreq=args.serve_requests, slots=args.serve_slots)
 
+    c1 = None
+    if world == 1 and not args.no_c1:
+        c1 = c1_leg(T, dev, max(3, min(args.steps, 10)), os.cpu_count() or 1, rank == 0)
+
+    plain = None
+    if world == 1 and not args.no_plain:
+        plain = plain_leg(T, dev, f, max(3, min(args.steps, 10)), rank == 0)
+
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu_leg(T, f, eb, B, dims, topo, sort, sizes, ctx)
@@ -866,6 +1051,8 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
+            "c1": c1,
+            "plain": plain,
             "e2e": e2e,
             "batched": batched,
             "served": served,

@@ -46,7 +46,7 @@ def build(ref: bool = True, ref_src: str | None = None) -> None:
     targets = ["oracle"]
     args = []
     if ref and src and os.path.isdir(os.path.join(src, "SZp")):
-        targets += ["ref", "refcuda"]
+        targets += ["ref", "refcpu2d", "refcuda"]
         args = ["REF=" + src]
     subprocess.run(["make", "-s", "-C", HERE] + args + targets, check=True)
 
@@ -395,6 +395,35 @@ def ref_decompress_sp(stream_after_count: bytes, e: int, B: int) -> np.ndarray:
     s = np.frombuffer(stream_after_count + b"\0" * 64, dtype=np.uint8).copy()
     ptr = reflib().szp_decompress_sort_positions(_p(s), e, B)
     return _take(ptr, 4 * e, np.int32)
+
+
+REF_CPU2D_SO = os.path.join(HERE, "_ref", "libszp_ref_cpu2d.so")
+_ref_cpu2d = None
+
+
+def ref_cpu2d_available() -> bool:
+    return os.path.exists(REF_CPU2D_SO)
+
+
+def ref_post_cpu2d(data, fn, sp, eb: float):
+    """The reference CPU decompress driver's own 2D post-processing sequence
+    (example/testfloat_decompress_fastmode1_topology.cc:826-966) on a copy of
+    data: returns (field, false-negative saddles, sigma, ksize, eps)."""
+    global _ref_cpu2d
+    if _ref_cpu2d is None:
+        L = C.CDLL(REF_CPU2D_SO)
+        L.ref2dcpu_post.restype = C.c_int
+        L.ref2dcpu_post.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_float,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_float)]
+        _ref_cpu2d = L
+    d = f32(data).copy()
+    t = np.ascontiguousarray(fn, dtype=np.int32)
+    s = None if sp is None or len(sp) == 0 else np.ascontiguousarray(sp, dtype=np.int32)
+    sig, ks, ep = C.c_double(0), C.c_int(0), C.c_float(0)
+    r, c = d.shape
+    fnc = _ref_cpu2d.ref2dcpu_post(_p(d), _p(t), _p(s), 0 if s is None else s.size, r, c, eb, C.byref(sig),
+                                   C.byref(ks), C.byref(ep))
+    return d, fnc, sig.value, ks.value, ep.value
 
 
 def ref_post(data, orig, fn, sp, eb: float, axis_stencil=False):

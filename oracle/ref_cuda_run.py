@@ -206,6 +206,58 @@ def _child(path, dims, eb, B, reps, warmup, dump):
     print(json.dumps(res))
 
 
+def _plain_child(path, n, dtype, eb, B, tb, reps, warmup):
+    x = np.fromfile(path, dtype=np.dtype(dtype), count=n)
+    L = C.CDLL(REF_CUDA_SO)
+    vp, sz, i = C.c_void_p, C.c_size_t, C.c_int
+    dbl = x.dtype == np.float64
+    ft = C.c_double if dbl else C.c_float
+    T = "double" if dbl else "float"
+    comp = getattr(L, "szp_cuda_%s_compress_%s" % (T, "threadblock" if tb else "randomaccess"))
+    comp.restype, comp.argtypes = vp, [vp, C.POINTER(sz), ft, sz, i]
+    dec = getattr(L, "szp_cuda_%s_decompress_%s_arg" % (T, "threadblock" if tb else "randomaccess"))
+    dec.restype, dec.argtypes = None, [vp, sz, ft, i, vp]
+    libc = C.CDLL(None)
+    libc.free.argtypes = [vp]
+    out = np.zeros(n, dtype=x.dtype)
+    tc, td = [], []
+    es = 8 if dbl else 4
+    for it in range(warmup + reps):
+        m = C.c_size_t(0)
+        t0 = time.perf_counter()
+        ptr = comp(x.ctypes.data_as(vp), C.byref(m), eb, n, B)
+        t1 = time.perf_counter()
+        s = C.string_at(ptr, m.value)
+        libc.free(ptr)
+        buf = np.zeros(len(s) - es + 4096, dtype=np.uint8)
+        buf[: len(s) - es] = np.frombuffer(s, dtype=np.uint8)[es:]
+        t2 = time.perf_counter()
+        dec(out.ctypes.data_as(vp), n, eb, B, buf.ctypes.data_as(vp))
+        t3 = time.perf_counter()
+        if it >= warmup:
+            tc.append((t1 - t0) * 1e3)
+            td.append((t3 - t2) * 1e3)
+    print(json.dumps({"bytes": len(s), "stream": sha(s), "values": sha(out.tobytes()),
+                      "ms": {"compress": statistics.median(tc), "decompress": statistics.median(td)}}))
+
+
+def run_plain(x: np.ndarray, eb: float, B: int, threadblock: bool = False, reps: int = 1, warmup: int = 0,
+              timeout: float = 1200.0) -> dict:
+    """The reference's CUDA plain codec (host-pointer compress, then its
+    decompressor on that stream) on a 1-D array, in a child process; digests
+    and median wall-clock milliseconds per call."""
+    d = np.ascontiguousarray(x)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "field.bin")
+        d.tofile(path)
+        cmd = [sys.executable, os.path.abspath(__file__), "--plain", path, str(d.size), d.dtype.str, repr(float(eb)),
+               str(B), str(int(threadblock)), str(reps), str(warmup)]
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    if p.returncode:
+        raise RuntimeError("reference CUDA plain run failed (%d): %s" % (p.returncode, p.stderr[-2000:]))
+    return json.loads(p.stdout.strip().splitlines()[-1])
+
+
 def run(field: np.ndarray, eb: float, B: int, reps: int = 1, warmup: int = 0, dump: str = None,
         timeout: float = 1200.0) -> dict:
     """The reference's CUDA path on `field` (fp32, 2D or 3D) in a child
@@ -224,5 +276,8 @@ def run(field: np.ndarray, eb: float, B: int, reps: int = 1, warmup: int = 0, du
 
 if __name__ == "__main__":
     a = sys.argv[1:]
+    if a and a[0] == "--plain":
+        _plain_child(a[1], int(a[2]), a[3], float(a[4]), int(a[5]), int(a[6]), int(a[7]), int(a[8]))
+        sys.exit(0)
     _child(a[0], [int(x) for x in a[1].split(",")], float(a[2]), int(a[3]), int(a[4]), int(a[5]),
            a[6] if len(a) > 6 and a[6] else None)
