@@ -366,6 +366,37 @@ SZP_B200_API int szp_b200_plain_decompress_dev(szp_b200_ctx *ctx, const unsigned
                                                int is_double, size_t n, double absErrBound, int blockSize,
                                                void *d_out);
 
+/* One field split across devices (no reference counterpart; the exchange
+ * steps run in the host layer, toposzp-cuda_b200/shard.py).  A slab
+ * [begin, end) of the field (block-aligned: begin and end multiples of 64, or
+ * end == n), held in d_slab from global element begin - halo_lo on (halo_lo a
+ * multiple of 4 covering min(begin, one plane + 1 -- one row + 1 in 2D), and
+ * the buffer reaching min(n, end + the same)), encodes into its topology
+ * blocks (no header; offsets relative to the slab) and its critical-point
+ * pairs {order-preserving value code, slab-local extremum index or ~0} in
+ * raster order.  blockSize 64.  Concatenated in slab order, the blocks of all
+ * slabs are the single-device topology payload. */
+typedef struct {
+    size_t payload_bytes;   /* topology blocks of the slab */
+    size_t cp_count;        /* critical points of the slab */
+    size_t extrema_count;   /* maxima + minima of the slab */
+} szp_b200_slab_sizes;
+SZP_B200_API int szp_b200_topo_encode_slab_dev(szp_b200_ctx *ctx, const float *d_slab, size_t halo_lo,
+                                               szp_b200_geom geom, float absErrBound, int blockSize,
+                                               size_t begin, size_t end, unsigned char *d_payload,
+                                               size_t payload_cap, void *d_pairs, size_t pairs_cap,
+                                               szp_b200_slab_sizes *sizes);
+/* Quantization bin (the reference's qbin of the value) of K pairs. */
+SZP_B200_API int szp_b200_pair_bins_dev(szp_b200_ctx *ctx, const void *d_pairs, size_t K, float absErrBound,
+                                        int *d_bins);
+/* Sort positions (dense rank of the value among the pairs of its bin) of the
+ * E extrema among K pairs, written at each pair's extremum index. */
+SZP_B200_API int szp_b200_rank_pairs_dev(szp_b200_ctx *ctx, const void *d_pairs, size_t K, size_t E,
+                                         float absErrBound, int *d_sp);
+/* [u64 0][blocks] of n ints (the sort-position stream format). */
+SZP_B200_API int szp_b200_encode_ints_dev(szp_b200_ctx *ctx, const int *d_vals, size_t n, int blockSize,
+                                          unsigned char *d_out, size_t out_cap, size_t *out_bytes);
+
 /* Bounded-wait self-test (no reference counterpart).  Every device wait of
  * the library gives up after a poll limit and reports an error instead of
  * hanging; this runs one such wait that can never be satisfied, with a short

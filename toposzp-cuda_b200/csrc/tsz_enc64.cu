@@ -78,7 +78,8 @@ __device__ __forceinline__ void e64_front(const Enc64Args &a, long long tile, un
   const int tid = threadIdx.x, lane = tid & 31;
   const int l = lane & 7, bi = tid >> 3;
   const long long n = (long long)a.n;
-  const long long i0 = tile * kE64Tile + 8 * tid;
+  const long long i0 = tile * kE64Tile + 8 * tid;   // local index of the octet
+  const long long g0 = (long long)a.base + i0;       // its global index
   const long long bstart = tile * kE64Tile + 64 * bi;
   const int len = bstart >= n ? 0 : (n - bstart >= 64 ? 64 : (int)(n - bstart));
   const int e0 = 8 * l;
@@ -87,12 +88,12 @@ __device__ __forceinline__ void e64_front(const Enc64Args &a, long long tile, un
   // ---- values of the octet ----
   float x[8];
   if (nv == 8) {
-    const float4 *px = reinterpret_cast<const float4 *>(a.data + i0);
+    const float4 *px = reinterpret_cast<const float4 *>(a.data + g0);
     const float4 u = __ldg(px), v = __ldg(px + 1);
     x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w; x[4] = v.x; x[5] = v.y; x[6] = v.z; x[7] = v.w;
   } else {
 #pragma unroll
-    for (int t = 0; t < 8; t++) x[t] = t < nv ? __ldg(a.data + i0 + t) : 0.f;
+    for (int t = 0; t < 8; t++) x[t] = t < nv ? __ldg(a.data + g0 + t) : 0.f;
   }
 
   // ---- interior mask: one coordinate split per octet ----
@@ -101,10 +102,10 @@ __device__ __forceinline__ void e64_front(const Enc64Args &a, long long tile, un
   if (nv > 0) {
     long long r, z0, y, xx = 0;
     if (D3) {
-      xx = fdivmod(i0, a.g.plane, a.g.m_plane, r);
+      xx = fdivmod(g0, a.g.plane, a.g.m_plane, r);
       y = fdivmod(r, a.g.d3, a.g.m_d3, z0);
     } else {
-      y = fdivmod(i0, a.g.d3, a.g.m_d3, z0);
+      y = fdivmod(g0, a.g.d3, a.g.m_d3, z0);
     }
     if (z0 + 7 < a.g.d3) {
       const bool row_in = y >= 1 && y <= a.g.d2 - 2 && (!D3 || (xx >= 1 && xx <= a.g.d1 - 2));
@@ -116,7 +117,7 @@ __device__ __forceinline__ void e64_front(const Enc64Args &a, long long tile, un
       inter &= (nv >= 8) ? 0xffu : ((1u << nv) - 1u);
     } else {
       wrap = true;   // the octet crosses a row: elements of several rows
-      inter = octet_interior(i0, nv, a.g);
+      inter = octet_interior(g0, nv, a.g);
     }
   }
 
@@ -125,8 +126,8 @@ __device__ __forceinline__ void e64_front(const Enc64Args &a, long long tile, un
   // consecutive elements); the warp's end lanes load their outer neighbour
   float prev = __shfl_up_sync(0xffffffffu, x[7], 1);
   float next = __shfl_down_sync(0xffffffffu, x[0], 1);
-  if (lane == 0 && (inter & 1u)) prev = __ldg(a.data + i0 - 1);
-  if (lane == 31 && (inter & 0x80u)) next = __ldg(a.data + i0 + 8);
+  if (lane == 0 && (inter & 1u)) prev = __ldg(a.data + g0 - 1);
+  if (lane == 31 && (inter & 0x80u)) next = __ldg(a.data + g0 + 8);
   unsigned types = 0, cpm = 0, exm = 0;
   if (__any_sync(0xffffffffu, inter != 0u)) {
     // edge j (0..8) joins element j-1 and j (element -1 = prev, 8 = next)
@@ -146,8 +147,8 @@ __device__ __forceinline__ void e64_front(const Enc64Args &a, long long tile, un
       // vector loads when the octet lies in one row and the offset keeps the
       // 16-byte alignment; per-element loads otherwise
       const long long oa = D3 ? a.g.plane : a.g.d3;
-      e64_axis(a.data, i0, oa, inter, !wrap && (oa & 3) == 0, x, ha, la);
-      if (D3) e64_axis(a.data, i0, a.g.d3, inter, !wrap && (a.g.d3 & 3) == 0, x, hb, lb);
+      e64_axis(a.data, g0, oa, inter, !wrap && (oa & 3) == 0, x, ha, la);
+      if (D3) e64_axis(a.data, g0, a.g.d3, inter, !wrap && (a.g.d3 & 3) == 0, x, hb, lb);
     }
     unsigned mx, mn, sd;
     if (D3) {
@@ -478,6 +479,8 @@ bool enc64_applies(const EncArgs &a, int mode) {
   return mode == kEncClassify && a.B == 64 && a.cp_mode == kCpPairs && a.out != nullptr &&
          (reinterpret_cast<uintptr_t>(a.data) & 15) == 0 && enc_tile_blocks(64) == kE64Blocks;
 }
+
+cudaError_t launch_enc64_args(const Enc64Args &a, cudaStream_t s, int sm_count) { return launch_enc64(a, s, sm_count); }
 
 cudaError_t launch_enc64_from(const EncArgs &e, cudaStream_t s, int sm_count) {
   Enc64Args a{};

@@ -21,6 +21,9 @@ struct Enc64Args {
   uint2 *cp_out;                // critical-point pairs {value code, extremum index or ~0}
   unsigned long long cp_cap;
   int spin_limit;               // look-back polls before giving up (0: default)
+  unsigned long long base;      // global index of local element 0 (a slab of a larger field; 0 otherwise):
+                                // tiles, blocks and outputs are local, classification and loads use
+                                // base + local through data (indexed by global element)
 };
 
 // The fused topology encoder with pairs output applies to blockSize 64 and a
@@ -28,6 +31,8 @@ struct Enc64Args {
 bool enc64_applies(const EncArgs &a, int mode);
 // Launches it over the tiles of a (persistent grid sized by occupancy).
 cudaError_t launch_enc64_from(const EncArgs &a, cudaStream_t s, int sm_count);
+cudaError_t launch_enc64_args(const Enc64Args &a, cudaStream_t s, int sm_count);
+unsigned long long enc64_tiles(unsigned long long n);
 
 // Bounded-wait checks (tests): a look-back whose predecessor never
 // publishes, and a grid barrier that one CTA never reaches.  Each returns 0

@@ -74,6 +74,10 @@ EXPORTS = [
     "szp_b200_plain_bound",
     "szp_b200_plain_compress_dev",
     "szp_b200_plain_decompress_dev",
+    "szp_b200_topo_encode_slab_dev",
+    "szp_b200_pair_bins_dev",
+    "szp_b200_rank_pairs_dev",
+    "szp_b200_encode_ints_dev",
     "szp_b200_selftest_bounded_wait",
     "szp_b200_container_bound",
     "szp_b200_container_from_streams_dev",
@@ -110,6 +114,10 @@ class Geom(C.Structure):
 class Sizes(C.Structure):
     _fields_ = [("topo_bytes", C.c_size_t), ("sort_bytes", C.c_size_t),
                 ("cp_count", C.c_size_t), ("extrema_count", C.c_size_t)]
+
+
+class SlabSizes(C.Structure):
+    _fields_ = [("payload_bytes", C.c_size_t), ("cp_count", C.c_size_t), ("extrema_count", C.c_size_t)]
 
 
 class ServerConfig(C.Structure):
@@ -222,6 +230,11 @@ def lib():
             "szp_cuda_float_decompress_threadblock_arg": (None, [vp, sz, f, i, vp]),
             "szp_cuda_double_decompress_threadblock": (vp, [sz, C.c_double, i, vp]),
             "szp_cuda_double_decompress_threadblock_arg": (None, [vp, sz, C.c_double, i, vp]),
+            "szp_b200_topo_encode_slab_dev": (i, [vp, vp, sz, Geom, f, i, sz, sz, vp, sz, vp, sz,
+                                                  C.POINTER(SlabSizes)]),
+            "szp_b200_pair_bins_dev": (i, [vp, vp, sz, f, vp]),
+            "szp_b200_rank_pairs_dev": (i, [vp, vp, sz, sz, f, vp]),
+            "szp_b200_encode_ints_dev": (i, [vp, vp, sz, i, vp, sz, C.POINTER(sz)]),
             "szp_b200_plain_bound": (sz, [sz, i, i, i]),
             "szp_b200_plain_compress_dev": (i, [vp, vp, i, sz, C.c_double, i, i, vp, sz, C.POINTER(sz)]),
             "szp_b200_plain_decompress_dev": (i, [vp, vp, sz, i, sz, C.c_double, i, vp]),
