@@ -37,7 +37,7 @@ encode_kernel(EncArgs a) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const unsigned FULL = 0xffffffffu;
-  const bool tags = (MODE != kEncInts);
+  const bool tags = mode_tags(MODE);
 
   uint32_t *scratch = reinterpret_cast<uint32_t *>(smem_dyn);            // kWarps * KMAX * 32
   unsigned char *img = smem_dyn + kWarps * KMAX * 32 * 4;                 // tile byte image
@@ -83,7 +83,7 @@ encode_kernel(EncArgs a) {
             const float x = a.data[base + j];
             qv = quantize(x, a.inv);
             if (MODE == kEncClassify) tv = (uint32_t)classify_at(a.data, base + j, a.g);
-            else tv = (uint32_t)(a.types[base + j] & 3u);
+            else if (MODE == kEncTypes) tv = (uint32_t)(a.types[base + j] & 3u);
           }
         }
         q[i][k] = qv;
@@ -520,7 +520,7 @@ size_t dec_smem_bytes(int B, bool tags) {
 template <int MODE, int KMAX, int BPW>
 static cudaError_t launch_enc(const EncArgs &a, cudaStream_t s, int grid) {
   auto k = encode_kernel<MODE, KMAX, BPW>;
-  const size_t sm = enc_smem_bytes(a.B, MODE != kEncInts);
+  const size_t sm = enc_smem_bytes(a.B, mode_tags(MODE));
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   k<<<grid, kThreads, sm, s>>>(a);
@@ -554,7 +554,7 @@ template <int MODE, int G>
 static cudaError_t launch_enc2(const EncArgs &a0, cudaStream_t s, int grid) {
   auto k = encode2_kernel<MODE, G>;
   EncArgs a = a0;
-  const size_t one = enc2_smem_bytes(a.B, MODE != kEncInts, MODE == kEncClassify);
+  const size_t one = enc2_smem_bytes(a.B, mode_tags(MODE), MODE == kEncClassify);
   // two tile images (pipelined look-back) unless the record CP mode is on
   const bool two = !(MODE == kEncClassify && a.cp_mode == kCpRecords);
   a.img_stride = two ? (unsigned)one : 0u;
@@ -584,11 +584,13 @@ cudaError_t launch_encode(int mode, const EncArgs &a, cudaStream_t s, int grid) 
     if (mode == kEncClassify) return launch_enc2_mode<kEncClassify>(a, s, grid);
     if (mode == kEncTypes) return launch_enc2_mode<kEncTypes>(a, s, grid);
     if (mode == kEncIntTypes) return launch_enc2_mode<kEncIntTypes>(a, s, grid);
+    if (mode == kEncQuant) return launch_enc2_mode<kEncQuant>(a, s, grid);
     return launch_enc2_mode<kEncInts>(a, s, grid);
   }
   if (mode == kEncClassify) return launch_enc_mode<kEncClassify>(a, s, grid);
   if (mode == kEncTypes) return launch_enc_mode<kEncTypes>(a, s, grid);
   if (mode == kEncIntTypes) return launch_enc_mode<kEncIntTypes>(a, s, grid);
+  if (mode == kEncQuant) return launch_enc_mode<kEncQuant>(a, s, grid);
   return launch_enc_mode<kEncInts>(a, s, grid);
 }
 

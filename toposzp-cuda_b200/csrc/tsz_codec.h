@@ -5,11 +5,15 @@
 namespace tsz {
 
 // kEncIntTypes: int values with per-element 2-bit tags (pre-quantized fields)
-enum EncMode { kEncClassify = 0, kEncTypes = 1, kEncInts = 2, kEncIntTypes = 3 };
+// kEncQuant: a float field quantized, no tags (the plain codec's blocks)
+enum EncMode { kEncClassify = 0, kEncTypes = 1, kEncInts = 2, kEncIntTypes = 3, kEncQuant = 4 };
+
+// whether the blocks of a mode carry 2-bit tags
+__host__ __device__ constexpr bool mode_tags(int mode) { return mode != kEncInts && mode != kEncQuant; }
 enum CpMode { kCpNone = 0, kCpRecords = 1, kCpPairs = 2 };
 
 struct EncArgs {
-  const float *data;            // float field (kEncClassify / kEncTypes)
+  const float *data;            // float field (kEncClassify / kEncTypes / kEncQuant)
   const int *ints;              // int values (kEncInts / kEncIntTypes)
   const unsigned char *types;   // per-element types 0..3 (kEncTypes / kEncIntTypes)
   unsigned long long n;

@@ -235,7 +235,7 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int gi = lane / G, l = lane % G;
-  const bool tags = (MODE != kEncInts);
+  const bool tags = mode_tags(MODE);
   const long long n = (long long)a.n;
   const int B = a.B;
   const long long nblocks = (n + B - 1) / B;
@@ -282,7 +282,7 @@ __device__ __forceinline__ void encode2_front(const EncArgs &a, const long long 
       for (int t = 0; t < 8; t++) if (t < nv) q[t] = quantize(x[t], a.inv);
       if (MODE == kEncClassify) {
         if (nv > 0) types = classify_octet(a.data, n, i0, nv, x, a.g, inter, ma, pa, mb, pb);
-      } else if (nv > 0) {
+      } else if (MODE == kEncTypes && nv > 0) {
         types = load_type_octet(a.types, i0, nv);
       }
     }
@@ -461,7 +461,7 @@ __device__ __forceinline__ void encode2_back(const EncArgs &a, const long long t
   constexpr int BPW = 32 / G;
   constexpr int TB = WARPS * BPW;
   uint32_t *s_bytes = sh.bytes;
-  const bool tags = (MODE != kEncInts);
+  const bool tags = mode_tags(MODE);
   uint32_t *imgw = reinterpret_cast<uint32_t *>(img);
   const long long n = (long long)a.n;
   const int B = a.B;

@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "tsz_ops.h"
@@ -506,7 +507,17 @@ static size_t plain_stream_bound(unsigned long long n, int B, int tb, size_t tsi
 
 static size_t plain_compress_scratch(unsigned long long n, int B, int tb) {
   const unsigned long long nb = plain_nblocks(n, B, tb);
-  return a256((nb + 1) * 8) + a256(scan_parts(nb + 1) * 8) + 1024;
+  const size_t two_pass = a256((nb + 1) * 8) + a256(scan_parts(nb + 1) * 8);
+  const size_t fused = B <= kMaxBlockSize ? a256((nb / enc_tile_blocks(B) + 2) * sizeof(TileDesc)) : 0;
+  return std::max(two_pass, fused) + 1024;
+}
+
+// Random-access float streams with blockSize <= 257 go through the fused
+// single-pass encoder (quantize-without-tags mode) and the octet decoder; the
+// block layout is the one the sort-position stream uses.
+template <class T>
+static bool plain_fused(int B, int tb) {
+  return std::is_same<T, float>::value && !tb && B <= kMaxBlockSize;
 }
 
 // The whole stream [T eb][u64 0][body] of d_data into d_out (device), on
@@ -518,6 +529,20 @@ static int plain_compress_impl(szp_b200_ctx *ctx, const T *d_data, unsigned long
   const unsigned long long nb = plain_nblocks(n, B, tb);
   const double inv = 1.0 / (double)eb;
   const unsigned long long hdr = sizeof(T) + 8, lead = tb ? 4 : 0;
+  if (plain_fused<T>(B, tb)) {
+    // [T eb] from the host, then the encoder's [u64 0][blocks] right behind it
+    memcpy(ctx->h_words + 16, &eb, sizeof(T));
+    if (out_cap < hdr ||
+        cuda_fail(cudaMemcpyAsync(d_out, ctx->h_words + 16, sizeof(T), cudaMemcpyHostToDevice, s), "H2D header"))
+      return out_cap < hdr ? (set_error("plain output buffer too small"), -1) : -1;
+    unsigned long long tot[3];
+    const Geom g = make_geom(2, 1, (long long)n, 1);
+    if (encode_pass(ctx, kEncQuant, reinterpret_cast<const float *>(d_data), nullptr, nullptr, n, B, (float)eb, g,
+                    d_out + sizeof(T), out_cap - sizeof(T), nullptr, kCpNone, nullptr, 0, tot))
+      return -1;
+    *out_len = hdr + tot[0];
+    return 0;
+  }
   unsigned long long *sizes = ctx->scratch.take<unsigned long long>(nb + 1);
   unsigned long long *part = ctx->scratch.take<unsigned long long>(scan_parts(nb + 1));
   if (!sizes || !part) { set_error("scratch arena too small"); return -1; }
@@ -554,6 +579,40 @@ static int plain_compress_impl(szp_b200_ctx *ctx, const T *d_data, unsigned long
   return 0;
 }
 
+// Random-access decode of a single-chunk payload whose block offsets are on
+// the device: the octet decoder for float streams (blockSize <= 256, or 257
+// on a 4-byte aligned payload), the warp-per-block decoder otherwise.
+template <class T>
+static int plain_decode_offsets(szp_b200_ctx *ctx, const unsigned char *pay, unsigned long long pay_len,
+                                const unsigned long long *offs, unsigned long long n, int B, T eb, T *d_out) {
+  cudaStream_t s = ctx->stream;
+  const unsigned long long nb = (n + B - 1) / B;
+  if (plain_fused<T>(B, 0) && (B <= 256 || (reinterpret_cast<uintptr_t>(pay) & 3u) == 0)) {
+    DecArgs a{};
+    a.payload = pay;
+    a.payload_len = pay_len;
+    a.blk_off = offs;
+    a.n = n;
+    a.B = B;
+    a.eb = (float)eb;
+    a.out_f = reinterpret_cast<float *>(d_out);
+    a.err = reinterpret_cast<int *>(ctx->d_words + 4);
+    if (cuda_fail(cudaMemsetAsync(ctx->d_words + 4, 0, 8, s), "memset") ||
+        cuda_fail(launch_decode(false, a, s), "plain decode launch"))
+      return -1;
+    ctx->launches += 1;
+    if (cuda_fail(cudaMemcpyAsync(ctx->h_words + 4, ctx->d_words + 4, 8, cudaMemcpyDeviceToHost, s), "D2H status") ||
+        cuda_fail(cudaStreamSynchronize(s), "plain decode"))
+      return -1;
+    if (ctx->h_words[4] & 0xffffffffu) { set_error("malformed plain stream (status %llu)", ctx->h_words[4]); return -1; }
+    return 0;
+  }
+  plain_decode_ra_kernel<T><<<plain_grid(ctx, nb), kPlainThreads, 0, s>>>(pay, nullptr, offs, n, B, nb, eb, d_out);
+  if (cuda_fail(cudaGetLastError(), "plain decode launch")) return -1;
+  ctx->launches += 1;
+  return cuda_fail(cudaStreamSynchronize(s), "plain decode") ? -1 : 0;
+}
+
 // Random-access decode of a single-chunk stream on the device (block offsets
 // parsed on the device).  d_in: the stream after its T header.
 template <class T>
@@ -573,11 +632,7 @@ static int plain_decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_i
       cuda_fail(cudaStreamSynchronize(s), "plain parse"))
     return -1;
   if (ctx->h_words[0] == 0 || ctx->h_words[1]) { set_error("malformed plain stream"); return -1; }
-  plain_decode_ra_kernel<T><<<plain_grid(ctx, nb), kPlainThreads, 0, s>>>(d_in + 8, nullptr, offs, n, B, nb, eb,
-                                                                          d_out);
-  if (cuda_fail(cudaGetLastError(), "plain decode launch")) return -1;
-  ctx->launches += 1;
-  return cuda_fail(cudaStreamSynchronize(s), "plain decode") ? -1 : 0;
+  return plain_decode_offsets<T>(ctx, d_in + 8, buf, offs, n, B, eb, d_out);
 }
 
 static bool plain_block_ok(int B, const char *fn) {
@@ -639,14 +694,24 @@ static void plain_decompress_host(const char *fn, T *h_out, size_t n, T eb, int 
   unsigned *d_part = ctx->scratch.take<unsigned>(scan_parts(nb + 1));
   T *d_out = ctx->scratch.take<T>(n);
   cudaStream_t s = ctx->stream;
+  const bool one_chunk_ra = !tb && Tn == 1;
   if (cuda_fail(cudaMemcpyAsync(d_s, cmp, L.end, cudaMemcpyHostToDevice, s), "H2D stream") ||
-      (nb && cuda_fail(cudaMemcpyAsync(d_desc, L.desc.data(), nb * sizeof(PlainDesc), cudaMemcpyHostToDevice, s),
-                       "H2D blocks")) ||
+      (nb && !one_chunk_ra &&
+       cuda_fail(cudaMemcpyAsync(d_desc, L.desc.data(), nb * sizeof(PlainDesc), cudaMemcpyHostToDevice, s),
+                 "H2D blocks")) ||
       (nc && cuda_fail(cudaMemcpyAsync(d_ch, L.chunks.data(), nc * sizeof(PlainChunk), cudaMemcpyHostToDevice, s),
                        "H2D chunks")))
     return;
   const unsigned char *pay = d_s + L.hdr;
-  if (!tb) {
+  if (one_chunk_ra) {
+    // one chunk: the compressors' regular block grid, payload offsets only
+    unsigned long long *d_off = reinterpret_cast<unsigned long long *>(d_desc);
+    std::vector<unsigned long long> offs(nb);
+    for (unsigned long long b = 0; b < nb; b++) offs[b] = L.desc[b].off;
+    if ((nb && cuda_fail(cudaMemcpyAsync(d_off, offs.data(), nb * 8, cudaMemcpyHostToDevice, s), "H2D offsets")) ||
+        plain_decode_offsets<T>(ctx, pay, L.end - L.hdr, d_off, n, B, eb, d_out))
+      return;
+  } else if (!tb) {
     plain_decode_ra_kernel<T><<<plain_grid(ctx, nb), kPlainThreads, 0, s>>>(pay, d_desc, nullptr, n, B, nb, eb, d_out);
     if (cuda_fail(cudaGetLastError(), "plain decode launch")) return;
     ctx->launches += 1;
