@@ -18,7 +18,10 @@
 //     earlier reads, so it cannot have been updated yet: F still holds its
 //     pre-pass value, exactly as in the serial pass.
 // Rounds repeat over the deferred items until none is left (their number is
-// the longest chain of adjacent candidates in raster order).  The raw decoded
+// the longest chain of adjacent candidates in raster order).  When the
+// stencil pass runs, enforcement is fused into it for every candidate with no
+// candidate face neighbour, and the enforcement pass proper runs only over the
+// rest (stencil_fused, enforce_sparse_kernel).  The raw decoded
 // value each point is clamped against is gathered per list entry when the
 // lists are built.  Floating-point expressions use explicit round-to-nearest
 // intrinsics so that no multiply-add is contracted (the reference host code is
@@ -84,6 +87,9 @@ struct PostArgs {
   int *err;
   unsigned *restored;
   int spin_limit;               // grid-barrier polls before giving up (0: default)
+  // stencil pass fused with enforcement (null: plain stencil pass): bitmap
+  // over list positions of the items that still need the enforcement pass
+  unsigned *NI;
 };
 
 __device__ __forceinline__ unsigned long long ld_rlx(const unsigned long long *p) {
@@ -257,9 +263,9 @@ __device__ __forceinline__ float enforce(const PostArgs &a, const Face &f, float
 // position (XP of its bitmap word plus the extrema before it in the word)
 // carries the value and the pass generation.  Returns false (nothing read is
 // used) while one of them is not final.  Every load is issued before the
-// first wait.
-template <int ND>
-__device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &f) {
+// first wait.  ISO: *iso tells whether no face neighbour of e is a candidate.
+template <int ND, bool ISO = false>
+__device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &f, bool *iso = nullptr) {
   const long long pl = a.g.plane, d3 = a.g.d3;
   // earlier neighbours k = 0 (x-1, 3D only), 1 (y-1), 2 (z-1): e is interior,
   // so each lies in the field
@@ -276,6 +282,17 @@ __device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &
     const unsigned b = (unsigned)(qb[k] & 31);
     cb[k] = (bw >> b) & 1u;
     pos[k] = base + (unsigned)__popc(bw & ((1u << b) - 1u));
+  }
+  if (ISO) {
+    // later neighbours x+1 (3D), y+1, z+1: inside the field, e being interior
+    const long long qa[3] = {e + pl, e + d3, e + 1};
+    unsigned later = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      if (ND == 2 && k == 0) continue;
+      later |= (a.X[qa[k] >> 5] >> (unsigned)(qa[k] & 31)) & 1u;
+    }
+    *iso = !(cb[0] || cb[1] || cb[2] || later);
   }
   unsigned long long wb[3];
   float fb[3];
@@ -700,25 +717,67 @@ __global__ void fn_detect_kernel(PostArgs a, const unsigned *__restrict__ Z, uns
   }
 }
 
+// Outcome of one item of a pass.
+enum { kItemDone = 0, kItemDeferred = 1, kItemNeedsEnforce = 2 };
+
+__device__ __forceinline__ float stencil_nd(const PostArgs &a, const Face &f, float cur, int t, int s, float o,
+                                            int nd) {
+  return nd == 2 ? stencil2(a, f, cur, t, s, o) : stencil3(a, f, t, s, o);
+}
+
+// The stencil pass fused with enforcement (a.NI set), item idx at point e.
+// The candidates split into the connected components of face adjacency, and
+// each pass reads, besides unchanged points, only the candidates of the
+// item's own component.  So a candidate with no candidate neighbour (three in
+// four on smooth fields) runs its enforcement right after its stencil, on the
+// same neighbour values, and stores only the final value (nothing reads its
+// result words).  The items of larger components run the stencil as usual
+// (result words, deferral) and report kItemNeedsEnforce; the enforcement pass
+// runs over them alone.
+template <int ND>
+__device__ __forceinline__ int stencil_fused(const PostArgs &a, unsigned idx, long long e) {
+  const float o = a.OL[idx];
+  const int t = ty(a, e);
+  const int s = idx < a.n_sp ? a.sp[idx] : 0;
+  const float cur = a.F[e];
+  Face f;
+  bool iso = false;
+  if (!read_face<ND, true>(a, e, f, &iso)) return kItemDeferred;
+  const float r = stencil_nd(a, f, cur, t, s, o, ND);
+  if (iso) {
+    a.F[e] = enforce<ND>(a, f, r, t, o);
+    return kItemDone;
+  }
+  a.F[e] = r;
+  st_rlx(&a.S[idx], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
+  return kItemNeedsEnforce;
+}
+
 // One item of a pass (list index idx): its result goes to S, or it is
-// deferred (returns true) while an earlier candidate it reads is not final.
+// deferred while an earlier candidate it reads is not final.  With a.NI set,
+// the stencil pass runs fused with enforcement (stencil_fused).
 template <int PASS, int ND>
-__device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx) {
+__device__ __forceinline__ int pass_item(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx) {
   const long long e = (long long)list[idx];
   float r;
   bool ok = false;
+  if (PASS == kPassStencil && a.NI) return stencil_fused<ND>(a, idx, e);
   if (PASS == kPassStencil || PASS == kPassEnforce) {
     const float o = a.OL[idx];
     const int t = ty(a, e);
     const int s = (PASS == kPassStencil && idx < a.n_sp) ? a.sp[idx] : 0;
     const float cur = a.F[e];
     Face f;
-    if (!read_face<ND>(a, e, f)) return true;
-    if (PASS == kPassStencil) r = (ND == 2) ? stencil2(a, f, cur, t, s, o) : stencil3(a, f, t, s, o);
-    else r = enforce<ND>(a, f, cur, t, o);
+    if (PASS == kPassStencil) {
+      if (!read_face<ND>(a, e, f)) return kItemDeferred;
+      r = (ND == 2) ? stencil2(a, f, cur, t, s, o) : stencil3(a, f, t, s, o);
+    } else {
+      if (!read_face<ND>(a, e, f)) return kItemDeferred;
+      r = enforce<ND>(a, f, cur, t, o);
+    }
   } else {
     const C3 c = coords(a.g, e);
-    if (!deps_ready<PASS, ND>(a, e, c)) return true;
+    if (!deps_ready<PASS, ND>(a, e, c)) return kItemDeferred;
     const float o = a.OL[idx];
     if (PASS == kPassRbf) {
       r = (ND == 2) ? rbf2(a, e, c, o, ok) : rbf3(a, e, c, o, ok);
@@ -734,7 +793,7 @@ __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__r
   a.F[e] = r;
   const long long sp = (PASS == kPassStencil || PASS == kPassEnforce) ? (long long)idx : e;
   st_rlx(&a.S[sp], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
-  return false;
+  return kItemDone;
 }
 
 // An item whose earlier candidate is handled by the same CTA at the same
@@ -742,7 +801,10 @@ __device__ __forceinline__ bool pass_item(const PostArgs &a, const unsigned *__r
 // deferred to the next round; the CTA instead retries its pending items a
 // few times, a block barrier apart, so that chains inside the CTA resolve in
 // this round.  Every thread of the CTA must call it.  Returns true while the
-// item is still pending.
+// item is still pending.  In the fused stencil pass, the items left for the
+// enforcement pass are marked in the a.NI bitmap here (one atomic per warp
+// when the warp's items share a bitmap word, as in a round over the whole
+// list).
 constexpr int kLocalRetries = 5;
 
 template <int PASS, int ND>
@@ -750,11 +812,32 @@ __device__ __forceinline__ bool pass_item_local(const PostArgs &a, const unsigne
                                                 bool valid) {
   // RBF and axis-pattern items are long and uneven: a block barrier would make
   // every thread wait for the slowest, so they retry in rounds only
-  if (PASS != kPassStencil && PASS != kPassEnforce) return valid && pass_item<PASS, ND>(a, list, idx);
-  bool pending = valid;
+  if (PASS != kPassStencil && PASS != kPassEnforce)
+    return valid && pass_item<PASS, ND>(a, list, idx) == kItemDeferred;
+  bool pending = valid, need = false;
   for (int it = 0; it < kLocalRetries; it++) {
-    if (pending) pending = pass_item<PASS, ND>(a, list, idx);
+    if (pending) {
+      const int st = pass_item<PASS, ND>(a, list, idx);
+      pending = st == kItemDeferred;
+      need = need || st == kItemNeedsEnforce;
+    }
     if (!__syncthreads_or(pending)) break;
+  }
+  if (PASS == kPassStencil && a.NI) {
+    const unsigned m = __ballot_sync(0xffffffffu, need);
+    if (m) {
+      const int lane = threadIdx.x & 31;
+      const int first = __ffs(m) - 1;
+      const unsigned wi = idx >> 5;
+      const unsigned w_first = __shfl_sync(0xffffffffu, wi, first);
+      const unsigned bit = need ? 1u << (idx & 31) : 0u;
+      if (__all_sync(0xffffffffu, !need || wi == w_first)) {
+        const unsigned bits = __reduce_or_sync(0xffffffffu, bit);
+        if (lane == first) atomicOr(&a.NI[w_first], bits);
+      } else if (need) {
+        atomicOr(&a.NI[wi], bit);
+      }
+    }
   }
   return pending;
 }
@@ -779,6 +862,55 @@ pass_round_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned 
   if (defer) Wn[base + __popc(m & ((1u << lane) - 1u))] = idx;
 }
 
+
+// Round 0 of the enforcement pass that follows the fused stencil pass: the
+// items are the set bits of the bitmap NI over list positions.  Each CTA
+// takes kSparseWords bitmap words (a window of the list in raster order),
+// gathers their set positions in shared memory in order and runs them as a
+// round does, so that neighbouring items still meet in one CTA and resolve
+// by its local retries.  Deferred items go to Wn.
+constexpr int kSparseWords = 24;
+
+template <int ND>
+__global__ void __launch_bounds__(kPostThreads, 8)
+enforce_sparse_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *__restrict__ NI,
+                      unsigned nwords, unsigned *__restrict__ Wn, unsigned *wn_count) {
+  __shared__ unsigned s_idx[kSparseWords * 32];
+  __shared__ unsigned s_total;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned w0 = blockIdx.x * kSparseWords;
+  if (warp == 0) {
+    const unsigned wi = w0 + lane;
+    unsigned bits = (lane < kSparseWords && wi < nwords) ? NI[wi] : 0u;
+    const unsigned c = __popc(bits);
+    unsigned incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    unsigned k = incl - c;   // < kSparseWords * 32: only the first kSparseWords lanes hold bits
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      s_idx[k++] = wi * 32u + (unsigned)b;
+    }
+    if (lane == 31) s_total = incl;
+  }
+  __syncthreads();
+  const unsigned total = s_total;
+  for (unsigned base = 0; base < total; base += kPostThreads) {
+    const unsigned i = base + threadIdx.x;
+    const bool valid = i < total;
+    const unsigned idx = valid ? s_idx[i] : 0u;
+    const bool defer = pass_item_local<kPassEnforce, ND>(a, list, idx, valid);
+    const unsigned m = __ballot_sync(0xffffffffu, defer);
+    unsigned wb = 0;
+    if (lane == 0 && m) wb = atomicAdd(wn_count, (unsigned)__popc(m));
+    wb = __shfl_sync(0xffffffffu, wb, 0);
+    if (defer) Wn[wb + __popc(m & ((1u << lane) - 1u))] = idx;
+  }
+}
 
 // A round over a worklist whose length is on the device (*nw_dev), in a
 // grid-stride loop over a grid of any size (no barrier inside).
@@ -1003,9 +1135,12 @@ unsigned long long *post_words(szp_b200_ctx *ctx, unsigned long long n) {
 // the scatter in one cooperative launch that reads its counts on the device.
 // Returns 1 when cooperative launch is not available (the caller then runs
 // the host-driven rounds).
+// ni_bits (enforcement after the fused stencil): round 0 runs over the set
+// bits of that bitmap of ni_words words instead of list / sel.
 template <int PASS, int ND>
 static int run_pass_coop(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, const unsigned *sel,
-                         unsigned count, const unsigned *count_dev, unsigned *W0, unsigned *W1) {
+                         unsigned count, const unsigned *count_dev, unsigned *W0, unsigned *W1,
+                         const unsigned *ni_bits = nullptr, unsigned ni_words = 0) {
   static int grid_for_dev[64];
   const int dev = ctx->device;
   if (dev < 0 || dev >= 64) return 1;
@@ -1037,10 +1172,15 @@ static int run_pass_coop(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, c
   if (!count_dev) {
     // rounds 0 and 1 as ordinary launches (all CTAs need not be resident:
     // the big rounds balance better this way), the rest cooperatively
-    if (count == 0) return 0;
+    if (count == 0 && !ni_bits) return 0;
+    if (ni_bits && ni_words == 0) return 0;
     if (cuda_fail(cudaMemsetAsync(n0, 0, 4, s), "memset")) return -1;
-    pass_round_kernel<PASS, ND><<<(count + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(a, list, sel,
-                                                                                                count, W0, n0);
+    if (ni_bits)
+      enforce_sparse_kernel<ND><<<(ni_words + kSparseWords - 1) / kSparseWords, kPostThreads, 0, s>>>(
+          a, list, ni_bits, ni_words, W0, n0);
+    else
+      pass_round_kernel<PASS, ND><<<(count + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(
+          a, list, sel, count, W0, n0);
     pass_round_dev_kernel<PASS, ND><<<ctx->sm_count * 8, kPostThreads, 0, s>>>(a, list, W0, n0, W1, n1);
     ctx->launches += 2;
     if (cuda_fail(cudaGetLastError(), "pass round")) return -1;
@@ -1130,12 +1270,36 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   a.OL = OX;
   a.X = Eb;
   if (a.sp && a.n_sp > 0) {
+    // stencil fused with enforcement; the items next to another candidate
+    // are marked in a bitmap over list positions (in R, unused until the
+    // lock dilation) and only they run the enforcement pass
+    const unsigned ni_words = (nx + 31) / 32;
+    unsigned *NIb = R;
+    if (cuda_fail(cudaMemsetAsync(NIb, 0, (size_t)ni_words * 4, s), "memset")) return -1;
     a.gen = next_gen(ctx);
+    a.NI = NIb;
     const int rc = run_pass_coop<kPassStencil, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
     if (rc < 0 || (rc > 0 && run_rounds<kPassStencil, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
+    a.NI = nullptr;
     tl_mark(ctx, "post_stencil");
-  }
-  {
+    a.gen = next_gen(ctx);
+    const int re = run_pass_coop<kPassEnforce, ND>(ctx, a, X, nullptr, 0, nullptr, W0, W1, NIb, ni_words);
+    if (re < 0) return -1;
+    if (re > 0 && ni_words) {
+      // host-driven rounds: the sparse round 0, then rounds over its deferred items
+      unsigned *cnt = reinterpret_cast<unsigned *>(ctx->d_words + 7);
+      unsigned left = 0;
+      if (cuda_fail(cudaMemsetAsync(cnt, 0, 4, s), "memset")) return -1;
+      enforce_sparse_kernel<ND><<<(ni_words + kSparseWords - 1) / kSparseWords, kPostThreads, 0, s>>>(
+          a, X, NIb, ni_words, Y, cnt);
+      ctx->launches += 1;
+      if (cuda_fail(cudaGetLastError(), "pass round") ||
+          cuda_fail(cudaMemcpyAsync(&left, cnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+          cuda_fail(cudaStreamSynchronize(s), "pass round"))
+        return -1;
+      if (left && run_rounds_sel<kPassEnforce, ND>(ctx, a, X, Y, left, W0, W1)) return -1;
+    }
+  } else {
     a.gen = next_gen(ctx);
     const int rc = run_pass_coop<kPassEnforce, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
     if (rc < 0 || (rc > 0 && run_rounds<kPassEnforce, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
