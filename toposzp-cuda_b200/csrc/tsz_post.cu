@@ -92,9 +92,13 @@ struct PostArgs {
   unsigned *NI;
 };
 
+// No "memory" clobber: a result word is read whole and carries its own
+// readiness, so these loads need no order with the other loads of an item, and
+// the compiler may issue them together (a clobber would serialise every load
+// after it behind the one before).  A retry re-reads after a barrier.
 __device__ __forceinline__ unsigned long long ld_rlx(const unsigned long long *p) {
   unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
   return v;
 }
 __device__ __forceinline__ void st_rlx(unsigned long long *p, unsigned long long v) {
@@ -161,29 +165,53 @@ __device__ __forceinline__ float valo(const PostArgs &a, long long e, const C3 &
   return a.F[q];
 }
 
+// value of the earlier point e + (dx, dy, dz) as the serial pass sees it,
+// with its loads issued whether or not the caller uses it (exists: the point
+// lies in the field; 0 otherwise)
+template <int PASS>
+__device__ __forceinline__ float far_back(const PostArgs &a, long long e, const C3 &c, int dx, int dy, int dz,
+                                          bool exists) {
+  if (!exists) return 0.f;
+  const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
+  const bool cand = is_cand_known<PASS>(a, q, interior_off(a, c, dx, dy, dz));
+  const float fv = a.F[q];
+  return cand ? __uint_as_float((unsigned)ld_rlx(&a.S[q])) : fv;
+}
+
 // every earlier candidate that an RBF / axis-pattern item may read has its
-// result for this pass
+// result for this pass: the earlier points of the 3x3(x3) box and the points
+// two steps back along each axis.  The candidate tests of all of them are
+// issued first, then the result words of the candidates, so an item waits
+// for two loads in a row, not one per point.
 template <int PASS, int ND>
 __device__ bool deps_ready(const PostArgs &a, long long e, const C3 &c) {
-  // RBF / axis pattern: earlier points of the 3x3(x3) box and the points two
-  // steps back along each axis
-  const int xr = (ND == 3) ? 1 : 0;
-  for (int dx = -xr; dx <= 0; dx++)
+  constexpr int NB = ND == 3 ? 13 : 4;   // earlier box points
+  long long q[NB + 3];
+  bool cand[NB + 3];
+  int k = 0;
+#pragma unroll
+  for (int dx = (ND == 3 ? -1 : 0); dx <= 0; dx++)
+#pragma unroll
     for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
       for (int dz = -1; dz <= 1; dz++) {
         if (dx == 0 && (dy > 0 || (dy == 0 && dz >= 0))) continue;
-        const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
-        if (is_cand_known<PASS>(a, q, interior_off(a, c, dx, dy, dz)) && !result_ready(a, q)) return false;
+        q[k] = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
+        cand[k] = is_cand_known<PASS>(a, q[k], interior_off(a, c, dx, dy, dz));
+        k++;
       }
-  const int far[3][3] = {{-2, 0, 0}, {0, -2, 0}, {0, 0, -2}};
-  for (int k = (ND == 3 ? 0 : 1); k < 3; k++) {
-    const int dx = far[k][0], dy = far[k][1], dz = far[k][2];
-    if (ND == 3 && c.x + dx < 0) continue;
-    if (c.y + dy < 0 || c.z + dz < 0) continue;
-    const long long q = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
-    if (is_cand_known<PASS>(a, q, interior_off(a, c, dx, dy, dz)) && !result_ready(a, q)) return false;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const int dx = j == 0 ? -2 : 0, dy = j == 1 ? -2 : 0, dz = j == 2 ? -2 : 0;
+    const bool in = (ND == 3 || j > 0) && c.x + dx >= 0 && c.y + dy >= 0 && c.z + dz >= 0;
+    q[NB + j] = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
+    cand[NB + j] = in && is_cand_known<PASS>(a, q[NB + j], interior_off(a, c, dx, dy, dz));
   }
-  return true;
+  bool ok = true;
+#pragma unroll
+  for (int i = 0; i < NB + 3; i++)
+    if (cand[i]) ok = ok & ((unsigned)(ld_rlx(&a.S[q[i]]) >> 32) == a.gen);
+  return ok;
 }
 
 // ----------------------------------------------------------------------------
@@ -371,10 +399,12 @@ __device__ float rbf2(const PostArgs &a, long long e, const C3 &c, float o, bool
   const bool vd = (c.y + 1 < rows - 1) && ty(a, e + cols) == 0;
   const bool vl = (c.z - 1 >= 1) && ty(a, e - 1) == 0;
   const bool vr = (c.z + 1 < cols - 1) && ty(a, e + 1) == 0;
-  const float u2 = vu ? valo<kPassRbf>(a, e, c, 0, -2, 0) : 0.f;
-  const float d2 = vd ? valo<kPassRbf>(a, e, c, 0, 2, 0) : 0.f;
-  const float l2 = vl ? valo<kPassRbf>(a, e, c, 0, 0, -2) : 0.f;
-  const float r2 = vr ? valo<kPassRbf>(a, e, c, 0, 0, 2) : 0.f;
+  // loaded wherever the points exist, so that the loads overlap
+  const float gu = far_back<kPassRbf>(a, e, c, 0, -2, 0, c.y >= 2);
+  const float gl = far_back<kPassRbf>(a, e, c, 0, 0, -2, c.z >= 2);
+  const float gd = c.y + 2 < rows ? a.F[e + 2 * cols] : 0.f;
+  const float gr = c.z + 2 < cols ? a.F[e + 2] : 0.f;
+  const float u2 = vu ? gu : 0.f, d2 = vd ? gd : 0.f, l2 = vl ? gl : 0.f, r2 = vr ? gr : 0.f;
   const float step = __fsub_rn(cand, old);
   float alpha = 1.0f;
   for (int it = 0; it < 10; it++) {
@@ -440,17 +470,48 @@ __device__ bool valid3(const PostArgs &a, long long e, const C3 &c, Win3 &W, flo
 // 3D RBF (example/test_cuda_topology_3d.cu:317-434).  Every value the
 // validation can read is loaded once into registers (compile-time indices):
 // the 3x3x3 box around e and the points two steps out along each axis, the
-// latter only where the serial code would read them (the neighbour on that
-// side is interior and regular).  A trial changes only the centre value.
+// latter loaded wherever they exist and used only where the serial code reads
+// them (the neighbour on that side is interior and regular).  The candidate
+// tests come first and every value load after them, so an item waits for a
+// few loads in a row, not one per point.  A trial changes only the centre
+// value.
 __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, float o, bool &ok) {
   ok = false;
   const float old = a.F[e];
   float v[27];   // box value at (dx, dy, dz): v[(dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)]
+  // which earlier box points (i < 13) are candidates, then every value: the
+  // result of an earlier candidate, else F (loads issued together)
+  bool cb[13];
+#pragma unroll
+  for (int i = 0; i < 13; i++) {
+    const int dx = i / 9 - 1, dy = (i / 3) % 3 - 1, dz = i % 3 - 1;
+    cb[i] = is_cand_known<kPassRbf>(a, e + dx * a.g.plane + dy * a.g.d3 + dz, interior_off(a, c, dx, dy, dz));
+  }
+#pragma unroll
+  for (int i = 0; i < 27; i++) {
+    const int dx = i / 9 - 1, dy = (i / 3) % 3 - 1, dz = i % 3 - 1;
+    const long long q = e + dx * a.g.plane + dy * a.g.d3 + dz;
+    v[i] = (i == 13) ? old : (i < 13 && cb[i]) ? __uint_as_float((unsigned)ld_rlx(&a.S[q])) : a.F[q];
+  }
+  // neighbours whose classification the validation checks, and their far sides
+  const long long pl = a.g.plane, d3 = a.g.d3;
+  const bool cxm = c.x - 1 >= 1 && ty(a, e - pl) == 0, cxp = c.x + 1 < a.g.d1 - 1 && ty(a, e + pl) == 0;
+  const bool cym = c.y - 1 >= 1 && ty(a, e - d3) == 0, cyp = c.y + 1 < a.g.d2 - 1 && ty(a, e + d3) == 0;
+  const bool czm = c.z - 1 >= 1 && ty(a, e - 1) == 0, czp = c.z + 1 < a.g.d3 - 1 && ty(a, e + 1) == 0;
+  // the far sides, loaded wherever they exist (not only after the type
+  // tests) so that their loads overlap; used as the serial pass reads them
+  const float gxm = far_back<kPassRbf>(a, e, c, -2, 0, 0, c.x >= 2);
+  const float gym = far_back<kPassRbf>(a, e, c, 0, -2, 0, c.y >= 2);
+  const float gzm = far_back<kPassRbf>(a, e, c, 0, 0, -2, c.z >= 2);
+  const float gxp = c.x + 2 < a.g.d1 ? a.F[e + 2 * pl] : 0.f;
+  const float gyp = c.y + 2 < a.g.d2 ? a.F[e + 2 * d3] : 0.f;
+  const float gzp = c.z + 2 < a.g.d3 ? a.F[e + 2] : 0.f;
+  const float fxm = cxm ? gxm : 0.f, fym = cym ? gym : 0.f, fzm = czm ? gzm : 0.f;
+  const float fxp = cxp ? gxp : 0.f, fyp = cyp ? gyp : 0.f, fzp = czp ? gzp : 0.f;
   double num = 0.0, den = 0.0;
 #pragma unroll
   for (int i = 0; i < 27; i++) {
     const int dx = i / 9 - 1, dy = (i / 3) % 3 - 1, dz = i % 3 - 1;
-    v[i] = (i == 13) ? old : valo<kPassRbf>(a, e, c, dx, dy, dz);
     double ww = c_w3[i];
     if (locked(a, e + dx * a.g.plane + dy * a.g.d3 + dz)) ww = __dmul_rn(ww, 0.4);
     num = __dadd_rn(num, __dmul_rn(ww, (double)v[i]));
@@ -462,17 +523,6 @@ __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, float o, bool
   float cand = __double2float_rn(__ddiv_rn(num, den));
   if (cand < lo) cand = lo;
   if (cand > hi) cand = hi;
-  // neighbours whose classification the validation checks, and their far sides
-  const long long pl = a.g.plane, d3 = a.g.d3;
-  const bool cxm = c.x - 1 >= 1 && ty(a, e - pl) == 0, cxp = c.x + 1 < a.g.d1 - 1 && ty(a, e + pl) == 0;
-  const bool cym = c.y - 1 >= 1 && ty(a, e - d3) == 0, cyp = c.y + 1 < a.g.d2 - 1 && ty(a, e + d3) == 0;
-  const bool czm = c.z - 1 >= 1 && ty(a, e - 1) == 0, czp = c.z + 1 < a.g.d3 - 1 && ty(a, e + 1) == 0;
-  const float fxm = cxm ? valo<kPassRbf>(a, e, c, -2, 0, 0) : 0.f;
-  const float fxp = cxp ? valo<kPassRbf>(a, e, c, 2, 0, 0) : 0.f;
-  const float fym = cym ? valo<kPassRbf>(a, e, c, 0, -2, 0) : 0.f;
-  const float fyp = cyp ? valo<kPassRbf>(a, e, c, 0, 2, 0) : 0.f;
-  const float fzm = czm ? valo<kPassRbf>(a, e, c, 0, 0, -2) : 0.f;
-  const float fzp = czp ? valo<kPassRbf>(a, e, c, 0, 0, 2) : 0.f;
 #define V3(dx, dy, dz) v[((dx) + 1) * 9 + ((dy) + 1) * 3 + ((dz) + 1)]
   const float step = __fsub_rn(cand, old);
   float alpha = 1.0f;
@@ -994,8 +1044,10 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, int spin_l
 // status: 0 done, 1 round limit, 2 no progress.
 constexpr int kCoopRoundLimit = 100000;
 
+// At least two CTAs per SM (128 registers): the long RBF items need the
+// resident threads more than registers.
 template <int PASS, int ND>
-__global__ void __launch_bounds__(kPostThreads)
+__global__ void __launch_bounds__(kPostThreads, 2)
 pass_coop_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *sel, unsigned total,
                  const unsigned *total_dev, const unsigned *W_start, const unsigned *nstart_dev, unsigned *Wx,
                  unsigned *Wy, unsigned *cnts, unsigned *bar, unsigned long long *status) {
