@@ -70,7 +70,11 @@ __constant__ double c_w3[27];
 
 struct PostArgs {
   float *F;                     // the field, updated in place
-  const float *OL;              // raw decoded value of each entry of the pass's list
+  // raw decoded value of each entry of the pass's list; null: the field is
+  // the decoded field itself, so an item's raw value is its own F value
+  // before its first write in the pass (F[e] changes only by e's own item)
+  const float *OL;
+  float *RAW;                   // fused stencil with OL null: raw values of the items left for enforcement
   unsigned char *T;             // types in bits 0..1
   const int *sp;
   unsigned long long n_sp;
@@ -598,15 +602,17 @@ __device__ float axis3(const PostArgs &a, long long e, const C3 &c, float o, boo
 // stored contiguously (X staged from the front of one buffer, Z from its back:
 // a point is in at most one list).  The last tile writes the totals to
 // tot[0] = (extrema << 32) | saddles.  The raw decoded value of every list
-// entry (O at its point) goes to OX / OZ beside it.
+// entry (Ox / Oz at its point) goes to OX / OZ beside it, for each list whose
+// source is given (none is needed when the passes read raw values from the
+// field itself).
 constexpr int kListPer = 32;
 constexpr int kListTile = kPostThreads * kListPer;
 
 __global__ void __launch_bounds__(kPostThreads)
 list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, TileDesc *desc, unsigned *tile_ctr,
                   int *err, unsigned *X, unsigned *Z, unsigned char *Eb, unsigned char *Ib,
-                  unsigned long long *tot, const float *__restrict__ O, float *OX, float *OZ,
-                  unsigned *XP) {
+                  unsigned long long *tot, const float *__restrict__ Ox, const float *__restrict__ Oz,
+                  float *OX, float *OZ, unsigned *XP) {
   __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
   __shared__ unsigned s_buf[kListTile];
   __shared__ long long s_tile;
@@ -710,14 +716,18 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
       }
 #pragma unroll
       for (int u = 0; u < 4; u++)
-        if (k0 + u * kPostThreads < te) v[u] = O[q[u]];
+        if (Ox && k0 + u * kPostThreads < te) v[u] = Ox[q[u]];
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const unsigned k = k0 + u * kPostThreads;
         if (k < te) {
           // a list position past n means corrupt tile offsets: recorded, not written
-          if (xb + k < (unsigned long long)n) { X[xb + k] = q[u]; OX[xb + k] = v[u]; }
-          else atomicExch(err, kErrMalformed);
+          if (xb + k < (unsigned long long)n) {
+            X[xb + k] = q[u];
+            if (Ox) OX[xb + k] = v[u];
+          } else {
+            atomicExch(err, kErrMalformed);
+          }
         }
       }
     }
@@ -731,13 +741,17 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
       }
 #pragma unroll
       for (int u = 0; u < 4; u++)
-        if (k0 + u * kPostThreads < ts) v[u] = O[q[u]];
+        if (Oz && k0 + u * kPostThreads < ts) v[u] = Oz[q[u]];
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const unsigned k = k0 + u * kPostThreads;
         if (k < ts) {
-          if (zb + k < (unsigned long long)n) { Z[zb + k] = q[u]; OZ[zb + k] = v[u]; }
-          else atomicExch(err, kErrMalformed);
+          if (zb + k < (unsigned long long)n) {
+            Z[zb + k] = q[u];
+            if (Oz) OZ[zb + k] = v[u];
+          } else {
+            atomicExch(err, kErrMalformed);
+          }
         }
       }
     }
@@ -786,10 +800,10 @@ __device__ __forceinline__ float stencil_nd(const PostArgs &a, const Face &f, fl
 // runs over them alone.
 template <int ND>
 __device__ __forceinline__ int stencil_fused(const PostArgs &a, unsigned idx, long long e) {
-  const float o = a.OL[idx];
   const int t = ty(a, e);
   const int s = idx < a.n_sp ? a.sp[idx] : 0;
   const float cur = a.F[e];
+  const float o = a.OL ? a.OL[idx] : cur;
   Face f;
   bool iso = false;
   if (!read_face<ND, true>(a, e, f, &iso)) return kItemDeferred;
@@ -798,6 +812,7 @@ __device__ __forceinline__ int stencil_fused(const PostArgs &a, unsigned idx, lo
     a.F[e] = enforce<ND>(a, f, r, t, o);
     return kItemDone;
   }
+  if (a.RAW) a.RAW[idx] = o;     // F[e] holds the stencil result from here on
   a.F[e] = r;
   st_rlx(&a.S[idx], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
   return kItemNeedsEnforce;
@@ -813,10 +828,10 @@ __device__ __forceinline__ int pass_item(const PostArgs &a, const unsigned *__re
   bool ok = false;
   if (PASS == kPassStencil && a.NI) return stencil_fused<ND>(a, idx, e);
   if (PASS == kPassStencil || PASS == kPassEnforce) {
-    const float o = a.OL[idx];
     const int t = ty(a, e);
     const int s = (PASS == kPassStencil && idx < a.n_sp) ? a.sp[idx] : 0;
     const float cur = a.F[e];
+    const float o = a.OL ? a.OL[idx] : cur;
     Face f;
     if (PASS == kPassStencil) {
       if (!read_face<ND>(a, e, f)) return kItemDeferred;
@@ -828,7 +843,7 @@ __device__ __forceinline__ int pass_item(const PostArgs &a, const unsigned *__re
   } else {
     const C3 c = coords(a.g, e);
     if (!deps_ready<PASS, ND>(a, e, c)) return kItemDeferred;
-    const float o = a.OL[idx];
+    const float o = a.OL ? a.OL[idx] : a.F[e];
     if (PASS == kPassRbf) {
       r = (ND == 2) ? rbf2(a, e, c, o, ok) : rbf3(a, e, c, o, ok);
     } else {
@@ -1315,11 +1330,14 @@ static int run_rounds_sel(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, 
 template <int ND>
 static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned nx, unsigned *Z, unsigned nz,
                           unsigned *Y, unsigned *W0, unsigned *W1, unsigned *R, unsigned *Lb,
-                          const unsigned *Eb, const unsigned *Ib, const float *OX, const float *OZ,
-                          int axis_stencil) {
+                          const unsigned *Eb, const unsigned *Ib, float *OX, const float *OZ,
+                          int axis_stencil, bool raw_in_F) {
   cudaStream_t s = ctx->stream;
   const long long n = a.n;
-  a.OL = OX;
+  // raw_in_F: OX / OZ were not gathered; OX keeps the raw values of the
+  // items the fused stencil leaves for enforcement
+  a.OL = raw_in_F ? nullptr : OX;
+  a.RAW = nullptr;
   a.X = Eb;
   if (a.sp && a.n_sp > 0) {
     // stencil fused with enforcement; the items next to another candidate
@@ -1330,9 +1348,12 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
     if (cuda_fail(cudaMemsetAsync(NIb, 0, (size_t)ni_words * 4, s), "memset")) return -1;
     a.gen = next_gen(ctx);
     a.NI = NIb;
+    a.RAW = raw_in_F ? OX : nullptr;
     const int rc = run_pass_coop<kPassStencil, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
     if (rc < 0 || (rc > 0 && run_rounds<kPassStencil, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
     a.NI = nullptr;
+    a.RAW = nullptr;
+    a.OL = OX;   // raw values of the remaining items (gathered, or stashed by the stencil)
     tl_mark(ctx, "post_stencil");
     a.gen = next_gen(ctx);
     const int re = run_pass_coop<kPassEnforce, ND>(ctx, a, X, nullptr, 0, nullptr, W0, W1, NIb, ni_words);
@@ -1383,8 +1404,9 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   if (cuda_fail(cudaGetLastError(), "fn detect")) return -1;
   tl_mark(ctx, "post_fn_locks");
   // RBF runs over Z restricted to the lost saddles (Y holds indices into Z);
-  // their number stays on the device
-  a.OL = OZ;
+  // their number stays on the device.  Saddles keep their raw values until
+  // RBF itself writes them.
+  a.OL = raw_in_F ? nullptr : OZ;
   a.gen = next_gen(ctx);
   const int rc = nz ? run_pass_coop<kPassRbf, ND>(ctx, a, Z, Y, 0, ycnt, W0, W1) : 0;
   if (rc < 0) return -1;
@@ -1397,6 +1419,7 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   }
   tl_mark(ctx, "post_rbf");
   if (axis_stencil && ND == 3 && nz) {
+    a.OL = OZ;   // gathered in every mode: RBF has changed some saddles
     a.gen = next_gen(ctx);
     const int ra = run_pass_coop<kPassAxis, ND>(ctx, a, Z, nullptr, nz, nullptr, W0, W1);
     if (ra < 0 || (ra > 0 && run_rounds<kPassAxis, ND>(ctx, a, Z, nz, W0, W1, nullptr))) return -1;
@@ -1439,11 +1462,17 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   unsigned long long *d_tot = w + 2;
   const long long ltiles = (n + kListTile - 1) / kListTile;
   if (cuda_fail(cudaMemsetAsync(desc, 0, (ltiles + 1) * sizeof(TileDesc), s), "memset")) return -1;
+  // post-processing of the decoded field itself: each item reads its raw
+  // value from F before it writes (no gathered raw lists), except the
+  // axis-pattern pass, which runs after RBF has changed saddles
+  const bool raw_in_F = d_orig == d_data;
+  const bool axis_raw = axis_stencil && g.nd == 3;
   {
     const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 6);
     list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
                                                     Z, reinterpret_cast<unsigned char *>(Eb),
-                                                    reinterpret_cast<unsigned char *>(Ib), d_tot, d_orig, OX, OZ, XP);
+                                                    reinterpret_cast<unsigned char *>(Ib), d_tot, raw_in_F ? nullptr : d_orig,
+                                                    raw_in_F && !axis_raw ? nullptr : d_orig, OX, OZ, XP);
   }
   ctx->launches += 1;
   unsigned long long tot = 0;
@@ -1467,8 +1496,10 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   a.err = reinterpret_cast<int *>(w + 4);
   a.restored = reinterpret_cast<unsigned *>(w + 5);
   const int rc = (g.nd == 2)
-                     ? run_all_passes<2>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, OX, OZ, axis_stencil)
-                     : run_all_passes<3>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, OX, OZ, axis_stencil);
+                     ? run_all_passes<2>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, OX, OZ, axis_stencil,
+                                         raw_in_F)
+                     : run_all_passes<3>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, OX, OZ, axis_stencil,
+                                         raw_in_F);
   if (rc) return -1;
   if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 96, cudaMemcpyDeviceToHost, s), "D2H") ||
       cuda_fail(cudaStreamSynchronize(s), "postprocess"))
