@@ -887,12 +887,11 @@ int decompress_dev_impl(szp_b200_ctx *ctx, const unsigned char *d_topo, size_t t
   unsigned long long *S = post_words(ctx, n);
   const unsigned long long ntiles = (n + 2047) / 2048;
   TileDesc *desc = A.take<TileDesc>(ntiles + 1);
-  unsigned *Lb = A.take<unsigned>((n + 31) / 32);
-  if (!S || !desc || !Lb) { set_error("scratch arena too small for post-processing"); return -1; }
+  if (!S || !desc) { set_error("scratch arena too small for post-processing"); return -1; }
   int restored = 0;
   // d_out holds the raw decoded field: the list build gathers the raw values
   // of the candidates from it before any pass updates it in place
-  return postprocess_with(ctx, d_out, d_out, T, S, desc, Lb, spp, spp ? E : 0, g, absErrBound,
+  return postprocess_with(ctx, d_out, d_out, T, S, desc, spp, spp ? E : 0, g, absErrBound,
                           postprocess == 2, &restored);
 }
 

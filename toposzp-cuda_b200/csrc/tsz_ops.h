@@ -63,7 +63,7 @@ int compact_extrema(szp_b200_ctx *ctx, const int *d_cps, int stride, unsigned lo
                     unsigned long long *E_out);
 unsigned long long *post_words(szp_b200_ctx *ctx, unsigned long long n);
 int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsigned char *d_T,
-                     unsigned long long *d_S, TileDesc *desc, unsigned *d_L, const int *d_sp,
+                     unsigned long long *d_S, TileDesc *desc, const int *d_sp,
                      unsigned long long n_sp, const Geom &g, float eb, int axis_stencil,
                      int *restored_out);
 

@@ -84,7 +84,6 @@ struct PostArgs {
   float eps;
   unsigned gen;                 // generation of the current pass
   unsigned long long *S;        // (generation << 32) | result bits, per point
-  const unsigned *L;            // lock bitmap: interior point next to an interior extremum
   const unsigned *R;            // RBF candidates (lost saddles) bitmap
   const unsigned *X;            // interior-extremum bitmap (the stencil / enforcement candidates)
   const unsigned *XP;           // per bitmap word: list position of its first extremum (X entries before it)
@@ -348,7 +347,55 @@ __device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &
   return true;
 }
 
-__device__ __forceinline__ bool locked(const PostArgs &a, long long q) { return bit_at(a.L, q); }
+// bits [b, b + 32) of a bitmap of nbits bits (zeros outside)
+__device__ __forceinline__ unsigned get32(const unsigned *__restrict__ bm, long long b, long long nbits) {
+  const long long w = b >> 5;  // arithmetic shift: floor for negative b
+  const unsigned sh = (unsigned)(b & 31);
+  const long long nw = (nbits + 31) >> 5;
+  const unsigned lo = (w >= 0 && w < nw) ? bm[w] : 0u;
+  const unsigned hi = (w + 1 >= 0 && w + 1 < nw) ? bm[w + 1] : 0u;
+  return sh ? __funnelshift_r(lo, hi, sh) : lo;
+}
+
+// Locks of the RBF box around e (example/test_cuda_topology.cu:229-242,
+// example/test_cuda_topology_3d.cu:325-341): box point q is locked when it is
+// interior and an interior extremum (a bit of the extremum bitmap a.X) lies
+// within Chebyshev distance 1 of it.  Read from the 5x5(x5) window of a.X
+// around e, one 5-bit row segment per row (z - 2 .. z + 2).  A segment that
+// runs past a row end reads points of the neighbouring row's boundary
+// columns, and a row outside the field reads boundary rows or nothing; none
+// of them holds an interior extremum, so the window needs no clipping.
+// Bit (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1) (dx = 0 in 2D: bit (dy + 1) * 3 + dz + 1).
+template <int ND>
+__device__ __forceinline__ unsigned box_locks(const PostArgs &a, long long e, const C3 &c) {
+  constexpr int NX = ND == 3 ? 5 : 1;
+  unsigned seg[NX][5];
+#pragma unroll
+  for (int i = 0; i < NX; i++)
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const long long b = e + (ND == 3 ? (long long)(i - 2) * a.g.plane : 0ll) + (long long)(j - 2) * a.g.d3 - 2;
+      seg[i][j] = get32(a.X, b, a.n) & 31u;
+    }
+  unsigned m = 0;
+#pragma unroll
+  for (int dx = (ND == 3 ? -1 : 0); dx <= (ND == 3 ? 1 : 0); dx++)
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++) {
+      unsigned acc = 0;
+#pragma unroll
+      for (int ox = (ND == 3 ? -1 : 0); ox <= (ND == 3 ? 1 : 0); ox++)
+#pragma unroll
+        for (int oy = -1; oy <= 1; oy++) acc |= seg[(ND == 3 ? dx + ox + 2 : 0)][dy + oy + 2];
+#pragma unroll
+      for (int dz = -1; dz <= 1; dz++) {
+        // window bits dz + 1 .. dz + 3 are the columns dz - 1 .. dz + 1
+        if (((acc >> (dz + 1)) & 7u) && interior_off(a, c, dx, dy, dz))
+          m |= 1u << ((ND == 3 ? (dx + 1) * 9 : 0) + (dy + 1) * 3 + (dz + 1));
+      }
+    }
+  return m;
+}
 
 __device__ __forceinline__ int cls4_eps(float c, float n, float s, float w, float e, float eps) {
   const float np = __fadd_rn(n, eps), sp = __fadd_rn(s, eps), wp = __fadd_rn(w, eps), ep = __fadd_rn(e, eps);
@@ -370,11 +417,12 @@ __device__ float rbf2(const PostArgs &a, long long e, const C3 &c, float o, bool
   for (int da = -1; da <= 1; da++)
     for (int db = -1; db <= 1; db++)
       v[da + 1][db + 1] = (da == 0 && db == 0) ? a.F[e] : valo<kPassRbf>(a, e, c, 0, da, db);
+  const unsigned lk = box_locks<2>(a, e, c);
   double num = 0.0, den = 0.0;
   for (int da = -1; da <= 1; da++)
     for (int db = -1; db <= 1; db++) {
       double ww = c_w2[(da + 1) * 3 + (db + 1)];
-      if (locked(a, e + da * cols + db)) ww = __dmul_rn(ww, 0.4);
+      if ((lk >> ((da + 1) * 3 + (db + 1))) & 1u) ww = __dmul_rn(ww, 0.4);
       num = __dadd_rn(num, __dmul_rn(ww, (double)v[da + 1][db + 1]));
       den = __dadd_rn(den, ww);
     }
@@ -512,12 +560,12 @@ __device__ float rbf3(const PostArgs &a, long long e, const C3 &c, float o, bool
   const float gzp = c.z + 2 < a.g.d3 ? a.F[e + 2] : 0.f;
   const float fxm = cxm ? gxm : 0.f, fym = cym ? gym : 0.f, fzm = czm ? gzm : 0.f;
   const float fxp = cxp ? gxp : 0.f, fyp = cyp ? gyp : 0.f, fzp = czp ? gzp : 0.f;
+  const unsigned lk = box_locks<3>(a, e, c);
   double num = 0.0, den = 0.0;
 #pragma unroll
   for (int i = 0; i < 27; i++) {
-    const int dx = i / 9 - 1, dy = (i / 3) % 3 - 1, dz = i % 3 - 1;
     double ww = c_w3[i];
-    if (locked(a, e + dx * a.g.plane + dy * a.g.d3 + dz)) ww = __dmul_rn(ww, 0.4);
+    if ((lk >> i) & 1u) ww = __dmul_rn(ww, 0.4);
     num = __dadd_rn(num, __dmul_rn(ww, (double)v[i]));
     den = __dadd_rn(den, ww);
   }
@@ -593,8 +641,8 @@ __device__ float axis3(const PostArgs &a, long long e, const C3 &c, float o, boo
 // candidate lists
 // ----------------------------------------------------------------------------
 
-// Interior extrema (X) and interior saddles (Z) in raster order plus the two
-// bitmaps (extrema Eb, interior Ib), in one pass over the types: persistent
+// Interior extrema (X) and interior saddles (Z) in raster order plus the
+// interior-extremum bitmap Eb, in one pass over the types: persistent
 // CTAs take tiles of kListTile points in order (32 consecutive points per
 // thread), publish their counts and find their list offsets by decoupled
 // look-back (extrema in the byte word, saddles in the count word), then write
@@ -610,7 +658,7 @@ constexpr int kListTile = kPostThreads * kListPer;
 
 __global__ void __launch_bounds__(kPostThreads)
 list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, TileDesc *desc, unsigned *tile_ctr,
-                  int *err, unsigned *X, unsigned *Z, unsigned char *Eb, unsigned char *Ib,
+                  int *err, unsigned *X, unsigned *Z, unsigned char *Eb,
                   unsigned long long *tot, const float *__restrict__ Ox, const float *__restrict__ Oz,
                   float *OX, float *OZ, unsigned *XP) {
   __shared__ unsigned s_w1[kWarps], s_w2[kWarps];
@@ -675,12 +723,8 @@ list_build_kernel(const unsigned char *__restrict__ T, Geom g, long long n, Tile
       // 4 bitmap bytes of this thread's 32 points (i0 is a multiple of 32)
       if (i0 + kListPer <= n) {
         reinterpret_cast<unsigned *>(Eb)[i0 >> 5] = em;
-        reinterpret_cast<unsigned *>(Ib)[i0 >> 5] = im;
       } else {
-        for (int k = 0; k < 4 && i0 + 8 * k < n; k++) {
-          Eb[(i0 >> 3) + k] = (unsigned char)(em >> (8 * k));
-          Ib[(i0 >> 3) + k] = (unsigned char)(im >> (8 * k));
-        }
+        for (int k = 0; k < 4 && i0 + 8 * k < n; k++) Eb[(i0 >> 3) + k] = (unsigned char)(em >> (8 * k));
       }
     }
     unsigned te, ts;
@@ -1109,36 +1153,6 @@ pass_coop_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *
   (void)tot;
 }
 
-// bits [b, b + 32) of a bitmap of nbits bits (zeros outside)
-__device__ __forceinline__ unsigned get32(const unsigned *__restrict__ bm, long long b, long long nbits) {
-  const long long w = b >> 5;  // arithmetic shift: floor for negative b
-  const unsigned sh = (unsigned)(b & 31);
-  const long long nw = (nbits + 31) >> 5;
-  const unsigned lo = (w >= 0 && w < nw) ? bm[w] : 0u;
-  const unsigned hi = (w + 1 >= 0 && w + 1 < nw) ? bm[w + 1] : 0u;
-  return sh ? __funnelshift_r(lo, hi, sh) : lo;
-}
-
-// lock bitmap: bit q set when q is interior and an interior extremum lies
-// within Chebyshev distance 1 (example/test_cuda_topology.cu:229-242,
-// example/test_cuda_topology_3d.cu:325-341): the interior-extremum bitmap E
-// dilated by one along every axis, masked by the interior bitmap I.  The
-// 3x3(x3) box is separable, so the dilation runs one axis at a time (flat
-// offsets 1, d3, d2*d3 become bit offsets; each output word ORs three shifted
-// 32-bit windows of the previous stage).  Points that wrap to another row or
-// plane lie on the boundary and are never interior extrema, so no dilated bit
-// crosses a row or plane edge.  I == nullptr: no mask (an intermediate axis).
-__global__ void dilate_bits_kernel(const unsigned *__restrict__ src, long long off, const unsigned *__restrict__ I,
-                                   long long n, unsigned *__restrict__ dst) {
-  const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nw = (n + 31) >> 5;
-  if (w >= nw) return;
-  const long long b0 = w << 5;
-  unsigned acc = src[w] | get32(src, b0 - off, n) | get32(src, b0 + off, n);
-  if (I) acc &= I[w];
-  dst[w] = acc;
-}
-
 __global__ void types_from_int_kernel(const int *__restrict__ fn, unsigned char *__restrict__ T, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) T[i] = (unsigned char)(fn[i] & 3);
@@ -1170,9 +1184,9 @@ static cudaError_t upload_weights(int dev) {
 size_t post_scratch_bytes(unsigned long long n) {
   const unsigned long long ntiles = (n + kPostTile - 1) / kPostTile;
   const unsigned long long words = (n + 31) / 32;
-  // T, descriptors, lock + RBF + extrema + interior bitmaps + extremum word
-  // positions, lists X and Z, worklists (2), Y, raw values of X and Z
-  return a256(n) + a256((ntiles + 1) * sizeof(TileDesc)) + 5 * a256(words * 4 + 4) + 7 * a256(n * 4) + 8192;
+  // T, descriptors, RBF + extrema bitmaps + extremum word positions, lists X
+  // and Z, worklists (2), Y, raw values of X and Z
+  return a256(n) + a256((ntiles + 1) * sizeof(TileDesc)) + 3 * a256(words * 4 + 4) + 7 * a256(n * 4) + 8192;
 }
 
 
@@ -1329,8 +1343,8 @@ static int run_rounds_sel(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, 
 
 template <int ND>
 static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned nx, unsigned *Z, unsigned nz,
-                          unsigned *Y, unsigned *W0, unsigned *W1, unsigned *R, unsigned *Lb,
-                          const unsigned *Eb, const unsigned *Ib, float *OX, const float *OZ,
+                          unsigned *Y, unsigned *W0, unsigned *W1, unsigned *R,
+                          const unsigned *Eb, float *OX, const float *OZ,
                           int axis_stencil, bool raw_in_F) {
   cudaStream_t s = ctx->stream;
   const long long n = a.n;
@@ -1342,7 +1356,7 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   if (a.sp && a.n_sp > 0) {
     // stencil fused with enforcement; the items next to another candidate
     // are marked in a bitmap over list positions (in R, unused until the
-    // lock dilation) and only they run the enforcement pass
+    // lost-saddle detection) and only they run the enforcement pass
     const unsigned ni_words = (nx + 31) / 32;
     unsigned *NIb = R;
     if (cuda_fail(cudaMemsetAsync(NIb, 0, (size_t)ni_words * 4, s), "memset")) return -1;
@@ -1378,26 +1392,12 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
     if (rc < 0 || (rc > 0 && run_rounds<kPassEnforce, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
   }
   tl_mark(ctx, "post_enforce");
-  // locks (static: from the types) and the lost saddles (from F after enforcement)
+  // the lost saddles (from F after enforcement); RBF reads the locks from the
+  // extremum bitmap (box_locks)
   const long long words = (n + 31) / 32;
-  {
-    // separable dilation of Eb: columns, rows, then planes (3D), with R as
-    // the scratch bitmap (cleared below), masked by Ib at the last axis
-    const unsigned gw = (unsigned)((words + 255) / 256);
-    if (ND == 2) {
-      dilate_bits_kernel<<<gw, 256, 0, s>>>(Eb, 1, nullptr, n, R);
-      dilate_bits_kernel<<<gw, 256, 0, s>>>(R, a.g.d3, Ib, n, Lb);
-    } else {
-      dilate_bits_kernel<<<gw, 256, 0, s>>>(Eb, 1, nullptr, n, Lb);
-      dilate_bits_kernel<<<gw, 256, 0, s>>>(Lb, a.g.d3, nullptr, n, R);
-      dilate_bits_kernel<<<gw, 256, 0, s>>>(R, a.g.plane, Ib, n, Lb);
-    }
-    ctx->launches += ND;
-  }
   if (cuda_fail(cudaMemsetAsync(R, 0, words * 4, s), "memset")) return -1;
   unsigned *ycnt = reinterpret_cast<unsigned *>(ctx->d_words + 8);
   if (cuda_fail(cudaMemsetAsync(ycnt, 0, 4, s), "memset")) return -1;
-  a.L = Lb;
   a.R = R;
   if (nz) fn_detect_kernel<<<(nz + 255) / 256, 256, 0, s>>>(a, Z, nz, R, Y, ycnt);
   ctx->launches += nz ? 1 : 0;
@@ -1429,7 +1429,7 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
 }
 
 int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsigned char *d_T,
-                     unsigned long long *d_S, TileDesc *desc, unsigned *d_L, const int *d_sp,
+                     unsigned long long *d_S, TileDesc *desc, const int *d_sp,
                      unsigned long long n_sp, const Geom &g, float eb, int axis_stencil, int *restored_out) {
   const long long n = g.d1 * g.d2 * g.d3;
   if (g.d2 < 3 || g.d3 < 3 || (g.nd == 3 && g.d1 < 3)) { if (restored_out) *restored_out = 0; return 0; }
@@ -1442,21 +1442,19 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   unsigned *X = A.take<unsigned>(n), *Z = A.take<unsigned>(n), *Y = A.take<unsigned>(n);
   unsigned *W0 = A.take<unsigned>(n), *W1 = A.take<unsigned>(n);
   unsigned *R = A.take<unsigned>((n + 31) / 32);
-  unsigned *Eb = A.take<unsigned>((n + 31) / 32 + 1), *Ib = A.take<unsigned>((n + 31) / 32 + 1);
+  unsigned *Eb = A.take<unsigned>((n + 31) / 32 + 1);
   unsigned *XP = A.take<unsigned>((n + 31) / 32 + 1);
   float *OX = A.take<float>(n), *OZ = A.take<float>(n);
-  if (!X || !Z || !Y || !W0 || !W1 || !R || !Eb || !Ib || !XP || !OX || !OZ) {
+  if (!X || !Z || !Y || !W0 || !W1 || !R || !Eb || !XP || !OX || !OZ) {
     set_error("scratch arena too small for post-processing");
     return -1;
   }
   unsigned long long *w = ctx->d_words;  // [9] pass status, [10] round counters
   if (cuda_fail(cudaMemsetAsync(w, 0, 96, s), "memset")) return -1;
   {
-    // the words past the last written byte of the two bitmaps must read as zero
+    // the words past the last written byte of the bitmap must read as zero
     const long long words = (n + 31) / 32;
-    if (cuda_fail(cudaMemsetAsync(Eb + words - 1, 0, 8, s), "memset") ||
-        cuda_fail(cudaMemsetAsync(Ib + words - 1, 0, 8, s), "memset"))
-      return -1;
+    if (cuda_fail(cudaMemsetAsync(Eb + words - 1, 0, 8, s), "memset")) return -1;
   }
   unsigned *tile_ctr = reinterpret_cast<unsigned *>(w + 3);
   unsigned long long *d_tot = w + 2;
@@ -1470,8 +1468,8 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   {
     const unsigned grid = (unsigned)std::min<long long>(ltiles, (long long)ctx->sm_count * 6);
     list_build_kernel<<<grid, kPostThreads, 0, s>>>(d_T, g, n, desc, tile_ctr, reinterpret_cast<int *>(w + 4), X,
-                                                    Z, reinterpret_cast<unsigned char *>(Eb),
-                                                    reinterpret_cast<unsigned char *>(Ib), d_tot, raw_in_F ? nullptr : d_orig,
+                                                    Z, reinterpret_cast<unsigned char *>(Eb), d_tot,
+                                                    raw_in_F ? nullptr : d_orig,
                                                     raw_in_F && !axis_raw ? nullptr : d_orig, OX, OZ, XP);
   }
   ctx->launches += 1;
@@ -1496,9 +1494,9 @@ int postprocess_with(szp_b200_ctx *ctx, float *d_data, const float *d_orig, unsi
   a.err = reinterpret_cast<int *>(w + 4);
   a.restored = reinterpret_cast<unsigned *>(w + 5);
   const int rc = (g.nd == 2)
-                     ? run_all_passes<2>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, OX, OZ, axis_stencil,
+                     ? run_all_passes<2>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, Eb, OX, OZ, axis_stencil,
                                          raw_in_F)
-                     : run_all_passes<3>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, d_L, Eb, Ib, OX, OZ, axis_stencil,
+                     : run_all_passes<3>(ctx, a, X, nx, Z, nz, Y, W0, W1, R, Eb, OX, OZ, axis_stencil,
                                          raw_in_F);
   if (rc) return -1;
   if (cuda_fail(cudaMemcpyAsync(ctx->h_words, w, 96, cudaMemcpyDeviceToHost, s), "D2H") ||
@@ -1554,8 +1552,7 @@ int postprocess(szp_b200_ctx *ctx, float *d_data, const float *d_orig,
   unsigned char *T = A.take<unsigned char>(n);
   const unsigned long long ntiles = (n + kPostTile - 1) / kPostTile;
   TileDesc *desc = A.take<TileDesc>(ntiles + 1);
-  unsigned *Lb = A.take<unsigned>((n + 31) / 32);
-  if (!S || !T || !desc || !Lb) { set_error("scratch arena too small for post-processing"); return -1; }
+  if (!S || !T || !desc) { set_error("scratch arena too small for post-processing"); return -1; }
   cudaStream_t s = ctx->stream;
   if (d_types_i) {
     types_from_int_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_types_i, T, n);
@@ -1563,7 +1560,7 @@ int postprocess(szp_b200_ctx *ctx, float *d_data, const float *d_orig,
   } else if (cuda_fail(cudaMemcpyAsync(T, d_types_u8, n, cudaMemcpyDeviceToDevice, s), "copy types")) {
     return -1;
   }
-  return postprocess_with(ctx, d_data, d_orig, T, S, desc, Lb, d_sp, n_sp, g, eb, axis_stencil, restored_out);
+  return postprocess_with(ctx, d_data, d_orig, T, S, desc, d_sp, n_sp, g, eb, axis_stencil, restored_out);
 }
 
 }  // namespace tsz
