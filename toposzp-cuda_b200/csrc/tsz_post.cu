@@ -21,7 +21,7 @@
 // the longest chain of adjacent candidates in raster order).  When the
 // stencil pass runs, enforcement is fused into it for every candidate with no
 // candidate face neighbour, and the enforcement pass proper runs only over the
-// rest (stencil_fused, enforce_sparse_kernel).  The raw decoded
+// rest (face_item_run, enforce_sparse_kernel).  The raw decoded
 // value each point is clamped against is gathered per list entry when the
 // lists are built.  Floating-point expressions use explicit round-to-nearest
 // intrinsics so that no multiply-add is contracted (the reference host code is
@@ -288,63 +288,81 @@ __device__ __forceinline__ float enforce(const PostArgs &a, const Face &f, float
   return (cur > tg) ? tg : cur;
 }
 
-// Reads the face neighbours of interior point e for a stencil / enforcement
-// item.  An earlier neighbour that is a candidate of the pass (an interior
-// extremum: a bit of X) must have its result already: the S word at its list
-// position (XP of its bitmap word plus the extrema before it in the word)
-// carries the value and the pass generation.  Returns false (nothing read is
-// used) while one of them is not final.  Every load is issued before the
-// first wait.  ISO: *iso tells whether no face neighbour of e is a candidate.
-template <int ND, bool ISO = false>
-__device__ __forceinline__ bool read_face(const PostArgs &a, long long e, Face &f, bool *iso = nullptr) {
+// An item of the stencil or enforcement pass, held in registers across the
+// local retries.  Its face neighbours as the serial pass sees them: the
+// earlier ones (x-1 in 3D, y-1, z-1) are results of this pass where they are
+// candidates (bits of X; the result word sits at the list position XP of the
+// bitmap word plus the extrema before it in the word), F otherwise; the
+// later ones are F.  Everything but the missing result words is loaded once;
+// a retry reloads only those.
+struct FaceItem {
+  long long e;
+  float cur, o;          // F at e before the item writes, and its raw value
+  int t, s;              // type, sort position (stencil)
+  Face f;
+  unsigned wait;         // bit k: earlier candidate neighbour k not read yet
+  unsigned pos[3];       // their list positions
+  bool iso;              // no face neighbour is a candidate (fused stencil)
+};
+
+template <int PASS, int ND>
+__device__ __forceinline__ void face_item_load(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx,
+                                               FaceItem &it) {
+  const long long e = (long long)list[idx];
   const long long pl = a.g.plane, d3 = a.g.d3;
-  // earlier neighbours k = 0 (x-1, 3D only), 1 (y-1), 2 (z-1): e is interior,
-  // so each lies in the field
-  const long long qb[3] = {e - pl, e - d3, e - 1};
-  bool cb[3];
-  unsigned pos[3];
+  it.e = e;
+  it.t = ty(a, e);
+  it.s = (PASS == kPassStencil && idx < a.n_sp) ? a.sp[idx] : 0;
+  it.cur = a.F[e];
+  it.o = a.OL ? a.OL[idx] : it.cur;
+  // e is interior: every face neighbour lies in the field
+  it.f.xm = ND == 3 ? a.F[e - pl] : 0.f;
+  it.f.xp = ND == 3 ? a.F[e + pl] : 0.f;
+  it.f.ym = a.F[e - d3];
+  it.f.yp = a.F[e + d3];
+  it.f.zm = a.F[e - 1];
+  it.f.zp = a.F[e + 1];
+  unsigned wait = 0;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    cb[k] = false;
-    pos[k] = 0;
+    it.pos[k] = 0;
     if (ND == 2 && k == 0) continue;
-    const long long wi = qb[k] >> 5;
-    const unsigned bw = a.X[wi], base = a.XP[wi];
-    const unsigned b = (unsigned)(qb[k] & 31);
-    cb[k] = (bw >> b) & 1u;
-    pos[k] = base + (unsigned)__popc(bw & ((1u << b) - 1u));
+    const long long q = e - (k == 0 ? pl : (k == 1 ? d3 : 1ll));
+    const long long wi = q >> 5;
+    const unsigned bw = a.X[wi], b = (unsigned)(q & 31);
+    wait |= ((bw >> b) & 1u) << k;
+    it.pos[k] = a.XP[wi] + (unsigned)__popc(bw & ((1u << b) - 1u));
   }
-  if (ISO) {
-    // later neighbours x+1 (3D), y+1, z+1: inside the field, e being interior
-    const long long qa[3] = {e + pl, e + d3, e + 1};
+  it.wait = wait;
+  it.iso = false;
+  if (PASS == kPassStencil && a.NI) {
     unsigned later = 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       if (ND == 2 && k == 0) continue;
-      later |= (a.X[qa[k] >> 5] >> (unsigned)(qa[k] & 31)) & 1u;
+      const long long q = e + (k == 0 ? pl : (k == 1 ? d3 : 1ll));
+      later |= (a.X[q >> 5] >> (unsigned)(q & 31)) & 1u;
     }
-    *iso = !(cb[0] || cb[1] || cb[2] || later);
+    it.iso = (wait | later) == 0u;
   }
-  unsigned long long wb[3];
-  float fb[3];
+}
+
+// Reads the result words still missing; false while one is not final.
+__device__ __forceinline__ bool face_item_ready(const PostArgs &a, FaceItem &it) {
+  unsigned long long w[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) w[k] = ((it.wait >> k) & 1u) ? ld_rlx(&a.S[it.pos[k]]) : 0ull;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    wb[k] = 0;
-    fb[k] = 0.f;
-    if (ND == 2 && k == 0) continue;
-    if (cb[k]) wb[k] = ld_rlx(&a.S[pos[k]]);
-    else fb[k] = a.F[qb[k]];
+    if (((it.wait >> k) & 1u) && (unsigned)(w[k] >> 32) == a.gen) {
+      const float v = __uint_as_float((unsigned)w[k]);
+      if (k == 0) it.f.xm = v;
+      else if (k == 1) it.f.ym = v;
+      else it.f.zm = v;
+      it.wait &= ~(1u << k);
+    }
   }
-  f.xp = (ND == 3) ? a.F[e + pl] : 0.f;
-  f.yp = a.F[e + d3];
-  f.zp = a.F[e + 1];
-#pragma unroll
-  for (int k = 0; k < 3; k++)
-    if (cb[k] && (unsigned)(wb[k] >> 32) != a.gen) return false;
-  f.xm = cb[0] ? __uint_as_float((unsigned)wb[0]) : fb[0];
-  f.ym = cb[1] ? __uint_as_float((unsigned)wb[1]) : fb[1];
-  f.zm = cb[2] ? __uint_as_float((unsigned)wb[2]) : fb[2];
-  return true;
+  return it.wait == 0u;
 }
 
 // bits [b, b + 32) of a bitmap of nbits bits (zeros outside)
@@ -842,66 +860,49 @@ __device__ __forceinline__ float stencil_nd(const PostArgs &a, const Face &f, fl
 // result words).  The items of larger components run the stencil as usual
 // (result words, deferral) and report kItemNeedsEnforce; the enforcement pass
 // runs over them alone.
-template <int ND>
-__device__ __forceinline__ int stencil_fused(const PostArgs &a, unsigned idx, long long e) {
-  const int t = ty(a, e);
-  const int s = idx < a.n_sp ? a.sp[idx] : 0;
-  const float cur = a.F[e];
-  const float o = a.OL ? a.OL[idx] : cur;
-  Face f;
-  bool iso = false;
-  if (!read_face<ND, true>(a, e, f, &iso)) return kItemDeferred;
-  const float r = stencil_nd(a, f, cur, t, s, o, ND);
-  if (iso) {
-    a.F[e] = enforce<ND>(a, f, r, t, o);
-    return kItemDone;
+template <int PASS, int ND>
+__device__ __forceinline__ int face_item_run(const PostArgs &a, unsigned idx, FaceItem &it) {
+  if (!face_item_ready(a, it)) return kItemDeferred;
+  const long long e = it.e;
+  float r;
+  int st = kItemDone;
+  if (PASS == kPassStencil) {
+    r = stencil_nd(a, it.f, it.cur, it.t, it.s, it.o, ND);
+    if (a.NI) {
+      if (it.iso) {
+        a.F[e] = enforce<ND>(a, it.f, r, it.t, it.o);
+        return kItemDone;
+      }
+      if (a.RAW) a.RAW[idx] = it.o;   // F[e] holds the stencil result from here on
+      st = kItemNeedsEnforce;
+    }
+  } else {
+    r = enforce<ND>(a, it.f, it.cur, it.t, it.o);
   }
-  if (a.RAW) a.RAW[idx] = o;     // F[e] holds the stencil result from here on
+  // in place: every reader of e's pre-pass value has finished (they are the
+  // earlier candidates e waited for); later readers take e's result from S
+  // at e's list position (dense, one coalesced word per item)
   a.F[e] = r;
   st_rlx(&a.S[idx], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
-  return kItemNeedsEnforce;
+  return st;
 }
 
-// One item of a pass (list index idx): its result goes to S, or it is
-// deferred while an earlier candidate it reads is not final.  With a.NI set,
-// the stencil pass runs fused with enforcement (stencil_fused).
+// One item of the RBF or axis-pattern pass (list index idx): its result goes
+// to F and to S at its point, or it is deferred while an earlier candidate it
+// reads is not final.
 template <int PASS, int ND>
 __device__ __forceinline__ int pass_item(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx) {
   const long long e = (long long)list[idx];
-  float r;
   bool ok = false;
-  if (PASS == kPassStencil && a.NI) return stencil_fused<ND>(a, idx, e);
-  if (PASS == kPassStencil || PASS == kPassEnforce) {
-    const int t = ty(a, e);
-    const int s = (PASS == kPassStencil && idx < a.n_sp) ? a.sp[idx] : 0;
-    const float cur = a.F[e];
-    const float o = a.OL ? a.OL[idx] : cur;
-    Face f;
-    if (PASS == kPassStencil) {
-      if (!read_face<ND>(a, e, f)) return kItemDeferred;
-      r = (ND == 2) ? stencil2(a, f, cur, t, s, o) : stencil3(a, f, t, s, o);
-    } else {
-      if (!read_face<ND>(a, e, f)) return kItemDeferred;
-      r = enforce<ND>(a, f, cur, t, o);
-    }
-  } else {
-    const C3 c = coords(a.g, e);
-    if (!deps_ready<PASS, ND>(a, e, c)) return kItemDeferred;
-    const float o = a.OL ? a.OL[idx] : a.F[e];
-    if (PASS == kPassRbf) {
-      r = (ND == 2) ? rbf2(a, e, c, o, ok) : rbf3(a, e, c, o, ok);
-    } else {
-      r = axis3(a, e, c, o, ok);
-    }
-  }
+  const C3 c = coords(a.g, e);
+  if (!deps_ready<PASS, ND>(a, e, c)) return kItemDeferred;
+  const float o = a.OL ? a.OL[idx] : a.F[e];
+  const float r = PASS == kPassRbf ? ((ND == 2) ? rbf2(a, e, c, o, ok) : rbf3(a, e, c, o, ok)) : axis3(a, e, c, o, ok);
   if (ok) atomicAdd(a.restored, 1u);
   // in place: every reader of e's pre-pass value has finished (they are the
-  // earlier candidates e waited for); later readers take e's result from S,
-  // at e's list position for the stencil / enforcement passes (dense, one
-  // coalesced word per item), at e itself for the RBF / axis passes
+  // earlier candidates e waited for); later readers take e's result from S
   a.F[e] = r;
-  const long long sp = (PASS == kPassStencil || PASS == kPassEnforce) ? (long long)idx : e;
-  st_rlx(&a.S[sp], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
+  st_rlx(&a.S[e], ((unsigned long long)a.gen << 32) | __float_as_uint(r));
   return kItemDone;
 }
 
@@ -924,9 +925,11 @@ __device__ __forceinline__ bool pass_item_local(const PostArgs &a, const unsigne
   if (PASS != kPassStencil && PASS != kPassEnforce)
     return valid && pass_item<PASS, ND>(a, list, idx) == kItemDeferred;
   bool pending = valid, need = false;
+  FaceItem item;
+  if (valid) face_item_load<PASS, ND>(a, list, idx, item);
   for (int it = 0; it < kLocalRetries; it++) {
     if (pending) {
-      const int st = pass_item<PASS, ND>(a, list, idx);
+      const int st = face_item_run<PASS, ND>(a, idx, item);
       pending = st == kItemDeferred;
       need = need || st == kItemNeedsEnforce;
     }
