@@ -982,18 +982,20 @@ pass_round_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned 
 // round does, so that neighbouring items still meet in one CTA and resolve
 // by its local retries.  Deferred items go to Wn.
 constexpr int kSparseWords = 24;
+static_assert(kSparseWords * 32 % kPostThreads == 0 && kSparseWords <= 32, "window of whole thread strides");
 
 template <int ND>
 __global__ void __launch_bounds__(kPostThreads, 8)
 enforce_sparse_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *__restrict__ NI,
                       unsigned nwords, unsigned *__restrict__ Wn, unsigned *wn_count) {
   __shared__ unsigned s_idx[kSparseWords * 32];
+  __shared__ unsigned s_word[kSparseWords], s_off[kSparseWords];
   __shared__ unsigned s_total;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned w0 = blockIdx.x * kSparseWords;
   if (warp == 0) {
     const unsigned wi = w0 + lane;
-    unsigned bits = (lane < kSparseWords && wi < nwords) ? NI[wi] : 0u;
+    const unsigned bits = (lane < kSparseWords && wi < nwords) ? NI[wi] : 0u;
     const unsigned c = __popc(bits);
     unsigned incl = c;
 #pragma unroll
@@ -1001,13 +1003,20 @@ enforce_sparse_kernel(PostArgs a, const unsigned *__restrict__ list, const unsig
       const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += u;
     }
-    unsigned k = incl - c;   // < kSparseWords * 32: only the first kSparseWords lanes hold bits
-    while (bits) {
-      const int b = __ffs(bits) - 1;
-      bits &= bits - 1;
-      s_idx[k++] = wi * 32u + (unsigned)b;
+    if (lane < kSparseWords) {
+      s_word[lane] = bits;
+      s_off[lane] = incl - c;
     }
     if (lane == 31) s_total = incl;
+  }
+  __syncthreads();
+  // every thread expands bit positions threadIdx.x + 256 j of the window, in
+  // order: position p goes to the slot of its word plus the set bits before it
+#pragma unroll
+  for (int j = 0; j < kSparseWords * 32 / kPostThreads; j++) {
+    const unsigned pbit = (unsigned)threadIdx.x + (unsigned)(j * kPostThreads);
+    const unsigned wd = s_word[pbit >> 5], b = pbit & 31u;
+    if ((wd >> b) & 1u) s_idx[s_off[pbit >> 5] + (unsigned)__popc(wd & ((1u << b) - 1u))] = w0 * 32u + pbit;
   }
   __syncthreads();
   const unsigned total = s_total;
