@@ -447,6 +447,12 @@ SZP_B200_API int szp_b200_batch_configure(szp_b200_batch *b, int use_graphs, int
  * Returns 0 on success. */
 SZP_B200_API int szp_b200_batch_compress(szp_b200_batch *b, szp_b200_batch_field *fields, int count);
 
+/* Sizes the batch's device and pinned buffers and its workspace for any batch
+ * of at most max_fields fields of at most max_elements elements in total, so
+ * that such batches allocate nothing (buffer growth frees memory, which waits
+ * for the whole device).  Returns 0 on success. */
+SZP_B200_API int szp_b200_batch_reserve(szp_b200_batch *b, int max_fields, size_t max_elements);
+
 /* Chosen shapes: shape[0..3] = topology encoder threads per CTA, CTAs per SM,
  * sort-position encoder threads per CTA, CTAs per SM; ms[] = the autotuner's
  * timings of the topology-encoder candidates.  Returns 1 once tuned. */
@@ -512,9 +518,11 @@ SZP_B200_API szp_b200_server *szp_b200_server_create(const szp_b200_server_confi
 SZP_B200_API void szp_b200_server_destroy(szp_b200_server *s);
 SZP_B200_API double szp_b200_server_now(szp_b200_server *s);
 /* Grows every worker's device workspace for requests of up to max_elements
- * elements, so that serving them allocates nothing (an allocation while
- * other workers run would stall the device for all of them).  Call it while
- * no request is in flight.  Returns 0 on success. */
+ * elements, and its batch compressor for the largest merged launch (up to
+ * max_batch fields of 2^24 elements in total), so that serving them allocates
+ * nothing (an allocation while other workers run would stall the device for
+ * all of them).  Call it while no request is in flight.  Returns 0 on
+ * success. */
 SZP_B200_API int szp_b200_server_reserve(szp_b200_server *s, size_t max_elements);
 SZP_B200_API int szp_b200_server_submit(szp_b200_server *s, szp_b200_request *r);
 /* 0 when r finished within timeout_s, 1 on timeout */

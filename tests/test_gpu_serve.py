@@ -186,3 +186,25 @@ def test_large_compressions_run_alone_and_match(T):
         assert got == ref
     assert all(arr[i].status == 0 for i in range(len(arr)))
     srv.close()
+
+
+def test_served_decompressions_match_single_workspace(T):
+    """Server workers run the post-processing rounds as ordinary launches in
+    bursts (their streams share the GPU, so no cooperative launch); the
+    decompressed fields equal those of a single workspace, whose round tails
+    run in one cooperative launch."""
+    import torch
+    spec, keep = build_mix(T, seed=7)
+    spec = [s for s in spec if s[0] == "d"]
+    assert len(spec) >= 4
+    srv = T.Server(slots=3, max_batch=8)
+    arr = to_requests(T, srv, spec)
+    srv.run_trace(arr)
+    ctx = T.Context()
+    for s, r in zip(spec, arr):
+        assert r.status == 0
+        _, dims, topo, tbytes, sort, sbytes, abs_eb, out = s
+        ref = ctx.decompress(topo, tbytes, sort if sbytes else None, sbytes, None, dims, abs_eb, 64, postprocess=1)
+        assert torch.equal(out.view(torch.int32), ref.view(torch.int32))
+    ctx.close()
+    srv.close()

@@ -742,6 +742,29 @@ int szp_b200_batch_tuning(szp_b200_batch *b, int *shape, float *ms, int max) {
 
 szp_b200_ctx *szp_b200_batch_ctx(szp_b200_batch *b) { return b ? b->ctx : nullptr; }
 
+int szp_b200_batch_reserve(szp_b200_batch *b, int max_fields, size_t max_elements) {
+  DeviceGuard dg(b ? b->ctx : nullptr);
+  clear_error();
+  if (!b || max_fields <= 0 || max_elements == 0) { set_error("szp_b200_batch_reserve: invalid arguments"); return -1; }
+  // bounds over any max_fields fields of max_elements elements in total
+  // (the sums szp_b200_batch_compress forms): blocks <= N / B + F, and a
+  // field's interior points (CP slots) <= its elements
+  const unsigned long long F = (unsigned long long)max_fields, N = max_elements, B = (unsigned long long)b->B;
+  const unsigned long long tb_min = (unsigned long long)tile_blocks_w(b->B, 4);
+  const unsigned long long blocks = N / B + F;
+  const unsigned long long tiles = blocks / tb_min + 2 * F + 1;
+  const unsigned long long itiles = N / B / tb_min + 3 * F + 1;
+  const int oldcap = b->cap_f;
+  const unsigned long long oldt = b->cap_tiles, oldp = b->cap_pairs, oldi = b->cap_itiles;
+  if (!batch_reserve(b, max_fields, tiles, N, itiles)) return -1;
+  if (b->cap_f != oldcap || b->cap_tiles != oldt || b->cap_pairs != oldp || b->cap_itiles != oldi) drop_graphs(b);
+  szp_b200_ctx *ctx = b->ctx;
+  if (!ctx->scratch.reserve(std::max(rank_scratch_bytes(N, ctx->sm_count),
+                                     rank_scratch_bytes_seg(N, max_fields, ctx->sm_count)) + 8192))
+    return -1;
+  return cuda_fail(cudaStreamSynchronize(ctx->stream), "batch reserve") ? -1 : 0;
+}
+
 int szp_b200_batch_compress(szp_b200_batch *b, szp_b200_batch_field *fs, int count) {
   DeviceGuard dg(b ? b->ctx : nullptr);
   clear_error();

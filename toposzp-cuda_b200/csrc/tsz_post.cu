@@ -1223,20 +1223,16 @@ unsigned long long *post_words(szp_b200_ctx *ctx, unsigned long long n) {
   return ctx->post_S;
 }
 
-// Runs one pass without host round trips: round 0 as one full-width launch
-// (when the item count is known on the host), then the remaining rounds and
-// the scatter in one cooperative launch that reads its counts on the device.
-// Returns 1 when cooperative launch is not available (the caller then runs
-// the host-driven rounds).
-// ni_bits (enforcement after the fused stencil): round 0 runs over the set
-// bits of that bitmap of ni_words words instead of list / sel.
+// Grid of the cooperative tail of pass PASS on this workspace's device (all
+// CTAs resident), or 0 when the workspace runs its tails as ordinary
+// launches: no cooperative launch on the device, or a workspace whose stream
+// shares the GPU with others (server workers), where a cooperative launch
+// can only start once all of its CTAs fit beside the other streams' kernels.
 template <int PASS, int ND>
-static int run_pass_coop(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, const unsigned *sel,
-                         unsigned count, const unsigned *count_dev, unsigned *W0, unsigned *W1,
-                         const unsigned *ni_bits = nullptr, unsigned ni_words = 0) {
+static int coop_grid(szp_b200_ctx *ctx) {
   static int grid_for_dev[64];
   const int dev = ctx->device;
-  if (dev < 0 || dev >= 64) return 1;
+  if (ctx->coop_off || dev < 0 || dev >= 64) return 0;
   if (grid_for_dev[dev] == 0) {
     int coop = 0, nb = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
@@ -1250,106 +1246,103 @@ static int run_pass_coop(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, c
       grid_for_dev[dev] = nb * ctx->sm_count;
     }
   }
-  if (grid_for_dev[dev] < 0) return 1;
+  return grid_for_dev[dev] > 0 ? grid_for_dev[dev] : 0;
+}
+
+// Rounds over deferred items as ordinary launches, kBurstRounds of them
+// between host checks of the remaining count: W holds the items on entry
+// (their count in word 7), W and Wo alternate.  Every round completes at
+// least the earliest pending item, so a burst that completes none reports an
+// error.
+constexpr int kBurstRounds = 4;
+constexpr int kRoundLimit = 100000;
+
+template <int PASS, int ND>
+static int finish_rounds(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, unsigned *W, unsigned *Wo) {
   cudaStream_t s = ctx->stream;
-  // words 10..13: three round counters, the barrier counter and generation,
-  // the length of the round-1 worklist
+  unsigned *c[3] = {reinterpret_cast<unsigned *>(ctx->d_words + 7), reinterpret_cast<unsigned *>(ctx->d_words + 11),
+                    reinterpret_cast<unsigned *>(ctx->d_words + 12)};
+  unsigned *h_left = reinterpret_cast<unsigned *>(ctx->h_words + 15);
+  int ci = 0;
+  unsigned prev = 0xffffffffu;
+  for (int r = 0; r < kRoundLimit; r += kBurstRounds) {
+    for (int k = 0; k < kBurstRounds; k++) {
+      unsigned *cn = c[(ci + 1) % 3];
+      if (cuda_fail(cudaMemsetAsync(cn, 0, 4, s), "memset")) return -1;
+      pass_round_dev_kernel<PASS, ND><<<ctx->sm_count * 4, kPostThreads, 0, s>>>(a, list, W, c[ci], Wo, cn);
+      std::swap(W, Wo);
+      ci = (ci + 1) % 3;
+    }
+    ctx->launches += kBurstRounds;
+    if (cuda_fail(cudaGetLastError(), "pass round") ||
+        cuda_fail(cudaMemcpyAsync(h_left, c[ci], 4, cudaMemcpyDeviceToHost, s), "D2H") ||
+        cuda_fail(cudaStreamSynchronize(s), "pass round"))
+      return -1;
+    const unsigned left = *h_left;
+    if (left == 0) return 0;
+    if (left >= prev) { set_error("post-processing pass made no progress"); return -1; }
+    prev = left;
+  }
+  set_error("post-processing pass did not converge");
+  return -1;
+}
+
+// Runs one pass: round 0 as one launch over all of its items -- list
+// positions 0 .. count-1, or sel[0 .. *count_dev) (count known only on the
+// device), or the set bits of the bitmap ni_bits of ni_words words (the
+// enforcement after the fused stencil) -- then the rounds over the deferred
+// items: in one cooperative launch that reads its counts on the device (after
+// one more ordinary round when round 0 ran over a list), or as bursts of
+// ordinary launches (finish_rounds).
+template <int PASS, int ND>
+static int run_pass(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, const unsigned *sel, unsigned count,
+                    const unsigned *count_dev, unsigned *W0, unsigned *W1, const unsigned *ni_bits = nullptr,
+                    unsigned ni_words = 0) {
+  if (ni_bits ? ni_words == 0 : (!count_dev && count == 0)) return 0;
+  const int grid = coop_grid<PASS, ND>(ctx);
+  cudaStream_t s = ctx->stream;
+  // words 7 (round-0 count) and 10..13: three round counters, the barrier
+  // counter and generation, the length of the round-1 worklist
+  unsigned *n0 = reinterpret_cast<unsigned *>(ctx->d_words + 7);
   unsigned *cnts = reinterpret_cast<unsigned *>(ctx->d_words + 10);
   unsigned *bar = cnts + 3;
   unsigned *n1 = cnts + 6;
-  unsigned *n0 = reinterpret_cast<unsigned *>(ctx->d_words + 7);
   unsigned long long *status = ctx->d_words + 9;
+  if (cuda_fail(cudaMemsetAsync(n0, 0, 4, s), "memset")) return -1;
+  if (ni_bits)
+    enforce_sparse_kernel<ND><<<(ni_words + kSparseWords - 1) / kSparseWords, kPostThreads, 0, s>>>(
+        a, list, ni_bits, ni_words, W0, n0);
+  else if (count_dev)
+    pass_round_dev_kernel<PASS, ND><<<ctx->sm_count * 2, kPostThreads, 0, s>>>(a, list, sel, count_dev, W0, n0);
+  else
+    pass_round_kernel<PASS, ND><<<(count + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(
+        a, list, sel, count, W0, n0);
+  ctx->launches += 1;
+  if (cuda_fail(cudaGetLastError(), "pass round")) return -1;
+  if (!grid) return finish_rounds<PASS, ND>(ctx, a, list, W0, W1);
   if (cuda_fail(cudaMemsetAsync(cnts, 0, 32, s), "memset")) return -1;
-  const unsigned *W_start = nullptr, *nstart = nullptr;
-  unsigned *Wx = W0, *Wy = W1;
+  const unsigned *W_start = W0, *nstart = n0;
+  unsigned *Wx = W1, *Wy = W0;
   if (!count_dev) {
-    // rounds 0 and 1 as ordinary launches (all CTAs need not be resident:
-    // the big rounds balance better this way), the rest cooperatively
-    if (count == 0 && !ni_bits) return 0;
-    if (ni_bits && ni_words == 0) return 0;
-    if (cuda_fail(cudaMemsetAsync(n0, 0, 4, s), "memset")) return -1;
-    if (ni_bits)
-      enforce_sparse_kernel<ND><<<(ni_words + kSparseWords - 1) / kSparseWords, kPostThreads, 0, s>>>(
-          a, list, ni_bits, ni_words, W0, n0);
-    else
-      pass_round_kernel<PASS, ND><<<(count + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(
-          a, list, sel, count, W0, n0);
+    // one more ordinary round (the round-0 remainder can still be large)
     pass_round_dev_kernel<PASS, ND><<<ctx->sm_count * 8, kPostThreads, 0, s>>>(a, list, W0, n0, W1, n1);
-    ctx->launches += 2;
+    ctx->launches += 1;
     if (cuda_fail(cudaGetLastError(), "pass round")) return -1;
     W_start = W1;
     nstart = n1;
     Wx = W0;
     Wy = W1;
   }
-  void *args[] = {(void *)&a,   (void *)&list,   (void *)&sel, (void *)&count, (void *)&count_dev,
-                  (void *)&W_start, (void *)&nstart, (void *)&Wx, (void *)&Wy, (void *)&cnts,
-                  (void *)&bar, (void *)&status};
-  if (cuda_fail(cudaLaunchCooperativeKernel((const void *)pass_coop_kernel<PASS, ND>, dim3(grid_for_dev[dev]),
-                                            dim3(kPostThreads), args, 0, s),
+  const unsigned zero = 0;
+  const unsigned *no_total = nullptr;
+  void *args[] = {(void *)&a,       (void *)&list,   (void *)&sel, (void *)&zero, (void *)&no_total,
+                  (void *)&W_start, (void *)&nstart, (void *)&Wx,  (void *)&Wy,   (void *)&cnts,
+                  (void *)&bar,     (void *)&status};
+  if (cuda_fail(cudaLaunchCooperativeKernel((const void *)pass_coop_kernel<PASS, ND>, dim3(grid), dim3(kPostThreads),
+                                            args, 0, s),
                 "cooperative pass launch"))
     return -1;
   ctx->launches += 1;
-  return 0;
-}
-
-// Runs one pass in rounds over `list` (count items); returns 0 on success.
-template <int PASS, int ND>
-static int run_rounds(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, unsigned count,
-                      unsigned *W0, unsigned *W1, const unsigned *sel_for_scatter) {
-  cudaStream_t s = ctx->stream;
-  unsigned *cnt = reinterpret_cast<unsigned *>(ctx->d_words + 7);
-  const unsigned *W = nullptr;  // round 0: every item
-  unsigned nw = count;
-  unsigned *bufs[2] = {W0, W1};
-  int b = 0;
-  for (int round = 0; nw > 0; round++) {
-    if (round > 100000) { set_error("post-processing pass did not converge"); return -1; }
-    if (cuda_fail(cudaMemsetAsync(cnt, 0, 4, s), "memset")) return -1;
-    pass_round_kernel<PASS, ND><<<(nw + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(
-        a, list, W, nw, bufs[b], cnt);
-    ctx->launches += 1;
-    unsigned next = 0;
-    if (cuda_fail(cudaGetLastError(), "pass round") ||
-        cuda_fail(cudaMemcpyAsync(&next, cnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
-        cuda_fail(cudaStreamSynchronize(s), "pass round"))
-      return -1;
-    if (next >= nw && round > 0) { set_error("post-processing pass made no progress"); return -1; }
-    W = bufs[b];
-    nw = next;
-    b ^= 1;
-  }
-  (void)sel_for_scatter;
-  return 0;
-}
-
-// rounds over list entries list[sel[i]], i < count (the RBF pass: lost saddles)
-template <int PASS, int ND>
-static int run_rounds_sel(szp_b200_ctx *ctx, PostArgs &a, const unsigned *list, const unsigned *sel,
-                          unsigned count, unsigned *W0, unsigned *W1) {
-  cudaStream_t s = ctx->stream;
-  // round 0 runs over sel itself (indices into list)
-  unsigned *cnt = reinterpret_cast<unsigned *>(ctx->d_words + 7);
-  const unsigned *W = sel;
-  unsigned nw = count;
-  unsigned *bufs[2] = {W0, W1};
-  int b = 0;
-  for (int round = 0; nw > 0; round++) {
-    if (round > 100000) { set_error("post-processing pass did not converge"); return -1; }
-    if (cuda_fail(cudaMemsetAsync(cnt, 0, 4, s), "memset")) return -1;
-    pass_round_kernel<PASS, ND><<<(nw + kPostThreads - 1) / kPostThreads, kPostThreads, 0, s>>>(
-        a, list, W, nw, bufs[b], cnt);
-    ctx->launches += 1;
-    unsigned next = 0;
-    if (cuda_fail(cudaGetLastError(), "pass round") ||
-        cuda_fail(cudaMemcpyAsync(&next, cnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
-        cuda_fail(cudaStreamSynchronize(s), "pass round"))
-      return -1;
-    if (next >= nw && round > 0) { set_error("post-processing pass made no progress"); return -1; }
-    W = bufs[b];
-    nw = next;
-    b ^= 1;
-  }
   return 0;
 }
 
@@ -1375,33 +1368,16 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
     a.gen = next_gen(ctx);
     a.NI = NIb;
     a.RAW = raw_in_F ? OX : nullptr;
-    const int rc = run_pass_coop<kPassStencil, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
-    if (rc < 0 || (rc > 0 && run_rounds<kPassStencil, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
+    if (run_pass<kPassStencil, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1)) return -1;
     a.NI = nullptr;
     a.RAW = nullptr;
     a.OL = OX;   // raw values of the remaining items (gathered, or stashed by the stencil)
     tl_mark(ctx, "post_stencil");
     a.gen = next_gen(ctx);
-    const int re = run_pass_coop<kPassEnforce, ND>(ctx, a, X, nullptr, 0, nullptr, W0, W1, NIb, ni_words);
-    if (re < 0) return -1;
-    if (re > 0 && ni_words) {
-      // host-driven rounds: the sparse round 0, then rounds over its deferred items
-      unsigned *cnt = reinterpret_cast<unsigned *>(ctx->d_words + 7);
-      unsigned left = 0;
-      if (cuda_fail(cudaMemsetAsync(cnt, 0, 4, s), "memset")) return -1;
-      enforce_sparse_kernel<ND><<<(ni_words + kSparseWords - 1) / kSparseWords, kPostThreads, 0, s>>>(
-          a, X, NIb, ni_words, Y, cnt);
-      ctx->launches += 1;
-      if (cuda_fail(cudaGetLastError(), "pass round") ||
-          cuda_fail(cudaMemcpyAsync(&left, cnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
-          cuda_fail(cudaStreamSynchronize(s), "pass round"))
-        return -1;
-      if (left && run_rounds_sel<kPassEnforce, ND>(ctx, a, X, Y, left, W0, W1)) return -1;
-    }
+    if (run_pass<kPassEnforce, ND>(ctx, a, X, nullptr, 0, nullptr, W0, W1, NIb, ni_words)) return -1;
   } else {
     a.gen = next_gen(ctx);
-    const int rc = run_pass_coop<kPassEnforce, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1);
-    if (rc < 0 || (rc > 0 && run_rounds<kPassEnforce, ND>(ctx, a, X, nx, W0, W1, nullptr))) return -1;
+    if (run_pass<kPassEnforce, ND>(ctx, a, X, nullptr, nx, nullptr, W0, W1)) return -1;
   }
   tl_mark(ctx, "post_enforce");
   // the lost saddles (from F after enforcement); RBF reads the locks from the
@@ -1420,21 +1396,12 @@ static int run_all_passes(szp_b200_ctx *ctx, PostArgs &a, unsigned *X, unsigned 
   // RBF itself writes them.
   a.OL = raw_in_F ? nullptr : OZ;
   a.gen = next_gen(ctx);
-  const int rc = nz ? run_pass_coop<kPassRbf, ND>(ctx, a, Z, Y, 0, ycnt, W0, W1) : 0;
-  if (rc < 0) return -1;
-  if (rc > 0) {
-    unsigned ny = 0;
-    if (cuda_fail(cudaMemcpyAsync(&ny, ycnt, 4, cudaMemcpyDeviceToHost, s), "D2H") ||
-        cuda_fail(cudaStreamSynchronize(s), "fn detect"))
-      return -1;
-    if (ny && run_rounds_sel<kPassRbf, ND>(ctx, a, Z, Y, ny, W0, W1)) return -1;
-  }
+  if (nz && run_pass<kPassRbf, ND>(ctx, a, Z, Y, 0, ycnt, W0, W1)) return -1;
   tl_mark(ctx, "post_rbf");
   if (axis_stencil && ND == 3 && nz) {
     a.OL = OZ;   // gathered in every mode: RBF has changed some saddles
     a.gen = next_gen(ctx);
-    const int ra = run_pass_coop<kPassAxis, ND>(ctx, a, Z, nullptr, nz, nullptr, W0, W1);
-    if (ra < 0 || (ra > 0 && run_rounds<kPassAxis, ND>(ctx, a, Z, nz, W0, W1, nullptr))) return -1;
+    if (run_pass<kPassAxis, ND>(ctx, a, Z, nullptr, nz, nullptr, W0, W1)) return -1;
     tl_mark(ctx, "post_axis");
   }
   return 0;

@@ -58,6 +58,9 @@ struct szp_b200_ctx {
   static constexpr int kChunkEvents = 16;
   cudaEvent_t chunk_ev[kChunkEvents] = {};   // parts of a chunked host-to-device copy
   cudaEvent_t part_ev[kChunkEvents] = {};    // encoder launches of a chunked encode
+  // no cooperative launches on this workspace's stream (set for server
+  // workers, whose streams share the GPU)
+  bool coop_off = false;
 };
 
 namespace tsz {

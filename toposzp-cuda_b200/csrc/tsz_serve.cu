@@ -118,6 +118,11 @@ static int compress_group(Slot &sl, szp_b200_request **rs, int count) {
 // and the single-field rank), and smaller ones are merged into batched
 // launches behind a small head.
 constexpr size_t kAloneElems = (size_t)1 << 21;
+// Elements of one merged launch at most: the workers' batch compressors are
+// sized for it up front (szp_b200_server_reserve), so serving allocates
+// nothing -- a buffer that grew would free memory, which waits for every
+// stream of the device.
+constexpr size_t kBatchElems = (size_t)1 << 24;
 
 static int compress_alone(Slot &sl, szp_b200_request *r) {
   float eb = r->errBound;
@@ -202,11 +207,14 @@ static void worker_main(szp_b200_server *S, int w) {
       if (grp[0].r->op == SZP_B200_OP_COMPRESS && elems_of(grp[0].r->geom) < kAloneElems) {
         // continuous batching: small compressions queued behind a small head
         // join its launch (large ones run alone on the fused path)
+        size_t elems = elems_of(grp[0].r->geom);
         for (auto it = S->q.begin(); it != S->q.end() && (int)grp.size() < S->cfg.max_batch;) {
-          if (it->r->op == SZP_B200_OP_COMPRESS && it->r->blockSize == grp[0].r->blockSize &&
-              elems_of(it->r->geom) < kAloneElems && bytes + it->cost <= batch_cap &&
+          const size_t ne = elems_of(it->r->geom);
+          if (it->r->op == SZP_B200_OP_COMPRESS && it->r->blockSize == grp[0].r->blockSize && ne < kAloneElems &&
+              elems + ne <= kBatchElems && bytes + it->cost <= batch_cap &&
               S->inflight_bytes + bytes + it->cost <= S->cfg.hbm_budget) {
             bytes += it->cost;
+            elems += ne;
             grp.push_back(*it);
             it = S->q.erase(it);
           } else {
@@ -265,6 +273,8 @@ szp_b200_server *szp_b200_server_create(const szp_b200_server_config *cfg) {
       break;
     }
     sl.ctx = szp_b200_ctx_create(sl.stream);
+    // the workers' streams share the GPU: no cooperative launches on them
+    if (sl.ctx) sl.ctx->coop_off = true;
     sl.batch = sl.ctx ? szp_b200_batch_create(sl.stream, cfg->blockSize) : nullptr;
     if (!sl.ctx || !sl.batch) { ok = false; break; }
   }
@@ -304,7 +314,9 @@ int szp_b200_server_reserve(szp_b200_server *S, size_t max_elements) {
     if (S->inflight || !S->q.empty()) { set_error("szp_b200_server_reserve: requests are in flight"); return -1; }
   }
   for (auto &sl : S->slots)
-    if (ctx_reserve_for(sl.ctx, max_elements, S->cfg.blockSize)) return -1;
+    if (ctx_reserve_for(sl.ctx, max_elements, S->cfg.blockSize) ||
+        szp_b200_batch_reserve(sl.batch, S->cfg.max_batch, kBatchElems))
+      return -1;
   return 0;
 }
 

@@ -86,6 +86,7 @@ EXPORTS = [
     "szp_b200_batch_destroy",
     "szp_b200_batch_configure",
     "szp_b200_batch_compress",
+    "szp_b200_batch_reserve",
     "szp_b200_batch_tuning",
     "szp_b200_batch_ctx",
     "szp_b200_server_create",
@@ -246,6 +247,7 @@ def lib():
             "szp_b200_batch_destroy": (None, [vp]),
             "szp_b200_batch_configure": (i, [vp, i, i]),
             "szp_b200_batch_compress": (i, [vp, C.POINTER(BatchField), i]),
+            "szp_b200_batch_reserve": (i, [vp, i, sz]),
             "szp_b200_batch_tuning": (i, [vp, C.POINTER(C.c_int), C.POINTER(C.c_float), i]),
             "szp_b200_batch_ctx": (vp, [vp]),
             "szp_b200_server_create": (vp, [C.POINTER(ServerConfig)]),
