@@ -377,7 +377,7 @@ bucket_rank_kernel(const uint2 *__restrict__ recs, BinSrc bin_of, const unsigned
 // (a new bin restarts at 0, every new distinct code adds 1).  Larger buckets
 // go on to the device-wide fallback.
 constexpr int kSortCap = 8192;
-constexpr int kSortThreads = 256;
+constexpr int kSortThreads = 1024;
 
 __global__ void __launch_bounds__(kSortThreads)
 bucket_sort_rank_kernel(const uint2 *__restrict__ recs, BinSrc bin_of, const unsigned long long *__restrict__ start,
