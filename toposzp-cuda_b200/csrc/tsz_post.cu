@@ -185,9 +185,14 @@ __device__ __forceinline__ float far_back(const PostArgs &a, long long e, const 
 // result for this pass: the earlier points of the 3x3(x3) box and the points
 // two steps back along each axis.  The candidate tests of all of them are
 // issued first, then the result words of the candidates, so an item waits
-// for two loads in a row, not one per point.
+// for two loads in a row, not one per point.  polls > 0: while a result is
+// missing, poll the missing words up to polls times (a bounded wait for
+// items of the same launch that are computing them); the item is deferred
+// when one is still missing.
+constexpr int kDepPolls = 256;
+
 template <int PASS, int ND>
-__device__ bool deps_ready(const PostArgs &a, long long e, const C3 &c) {
+__device__ bool deps_ready(const PostArgs &a, long long e, const C3 &c, int polls = 0) {
   constexpr int NB = ND == 3 ? 13 : 4;   // earlier box points
   long long q[NB + 3];
   bool cand[NB + 3];
@@ -210,11 +215,17 @@ __device__ bool deps_ready(const PostArgs &a, long long e, const C3 &c) {
     q[NB + j] = e + (long long)dx * a.g.plane + (long long)dy * a.g.d3 + dz;
     cand[NB + j] = in && is_cand_known<PASS>(a, q[NB + j], interior_off(a, c, dx, dy, dz));
   }
-  bool ok = true;
+  unsigned pend = 0;
 #pragma unroll
   for (int i = 0; i < NB + 3; i++)
-    if (cand[i]) ok = ok & ((unsigned)(ld_rlx(&a.S[q[i]]) >> 32) == a.gen);
-  return ok;
+    if (cand[i] && (unsigned)(ld_rlx(&a.S[q[i]]) >> 32) != a.gen) pend |= 1u << i;
+  for (int p = 0; pend && p < polls; p++) {
+    __nanosleep(256);
+#pragma unroll
+    for (int i = 0; i < NB + 3; i++)
+      if (((pend >> i) & 1u) && (unsigned)(ld_rlx(&a.S[q[i]]) >> 32) == a.gen) pend &= ~(1u << i);
+  }
+  return pend == 0;
 }
 
 // ----------------------------------------------------------------------------
@@ -891,11 +902,12 @@ __device__ __forceinline__ int face_item_run(const PostArgs &a, unsigned idx, Fa
 // to F and to S at its point, or it is deferred while an earlier candidate it
 // reads is not final.
 template <int PASS, int ND>
-__device__ __forceinline__ int pass_item(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx) {
+__device__ __forceinline__ int pass_item(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx,
+                                         int polls) {
   const long long e = (long long)list[idx];
   bool ok = false;
   const C3 c = coords(a.g, e);
-  if (!deps_ready<PASS, ND>(a, e, c)) return kItemDeferred;
+  if (!deps_ready<PASS, ND>(a, e, c, polls)) return kItemDeferred;
   const float o = a.OL ? a.OL[idx] : a.F[e];
   const float r = PASS == kPassRbf ? ((ND == 2) ? rbf2(a, e, c, o, ok) : rbf3(a, e, c, o, ok)) : axis3(a, e, c, o, ok);
   if (ok) atomicAdd(a.restored, 1u);
@@ -919,11 +931,12 @@ constexpr int kLocalRetries = 5;
 
 template <int PASS, int ND>
 __device__ __forceinline__ bool pass_item_local(const PostArgs &a, const unsigned *__restrict__ list, unsigned idx,
-                                                bool valid) {
+                                                bool valid, int polls = 0) {
   // RBF and axis-pattern items are long and uneven: a block barrier would make
-  // every thread wait for the slowest, so they retry in rounds only
+  // every thread wait for the slowest, so they wait for missing results on
+  // their own (bounded, polls) or retry in rounds
   if (PASS != kPassStencil && PASS != kPassEnforce)
-    return valid && pass_item<PASS, ND>(a, list, idx) == kItemDeferred;
+    return valid && pass_item<PASS, ND>(a, list, idx, polls) == kItemDeferred;
   bool pending = valid, need = false;
   FaceItem item;
   if (valid) face_item_load<PASS, ND>(a, list, idx, item);
@@ -1042,11 +1055,14 @@ pass_round_dev_kernel(PostArgs a, const unsigned *__restrict__ list, const unsig
   const unsigned nw = *nw_dev;
   const int lane = threadIdx.x & 31;
   const unsigned stride = gridDim.x * blockDim.x;
+  // every item of the round in flight at once: an item may wait for the
+  // earlier ones it reads, which are being computed beside it
+  const int polls = nw <= stride ? kDepPolls : 0;
   for (unsigned base = blockIdx.x * blockDim.x; base < nw; base += stride) {
     const unsigned i = base + threadIdx.x;
     unsigned idx = 0;
     if (i < nw) idx = W[i];
-    const bool defer = pass_item_local<PASS, ND>(a, list, idx, i < nw);
+    const bool defer = pass_item_local<PASS, ND>(a, list, idx, i < nw, polls);
     const unsigned m = __ballot_sync(0xffffffffu, defer);
     unsigned wb = 0;
     if (lane == 0 && m) wb = atomicAdd(wn_count, (unsigned)__popc(m));
@@ -1145,7 +1161,7 @@ pass_coop_kernel(PostArgs a, const unsigned *__restrict__ list, const unsigned *
       const unsigned i = base + threadIdx.x;
       unsigned idx = 0;
       if (i < nw) idx = W ? __ldcg(W + i) : i;
-      const bool defer = pass_item_local<PASS, ND>(a, list, idx, i < nw);
+      const bool defer = pass_item_local<PASS, ND>(a, list, idx, i < nw, nw <= stride ? kDepPolls : 0);
       const unsigned m = __ballot_sync(0xffffffffu, defer);
       unsigned wb = 0;
       if (lane == 0 && m) wb = atomicAdd(cnt, (unsigned)__popc(m));
