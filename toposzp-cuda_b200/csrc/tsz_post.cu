@@ -12,7 +12,9 @@
 //     S[e] = (generation << 32) | float bits: one 64-bit word that a reader
 //     takes whole (relaxed), so value and readiness never need ordering;
 //   * a candidate is computed once every EARLIER candidate it reads has its
-//     result for this pass (read from S); otherwise it is deferred to the
+//     result for this pass (read from S); otherwise it is retried (stencil
+//     and enforcement: a few times, a CTA barrier apart; RBF and axis
+//     pattern: bounded polls of the missing words) and then deferred to the
 //     next round;
 //   * every LATER point a candidate reads lists that candidate among its own
 //     earlier reads, so it cannot have been updated yet: F still holds its
@@ -21,9 +23,10 @@
 // the longest chain of adjacent candidates in raster order).  When the
 // stencil pass runs, enforcement is fused into it for every candidate with no
 // candidate face neighbour, and the enforcement pass proper runs only over the
-// rest (face_item_run, enforce_sparse_kernel).  The raw decoded
-// value each point is clamped against is gathered per list entry when the
-// lists are built.  Floating-point expressions use explicit round-to-nearest
+// rest (face_item_run, enforce_sparse_kernel).  The raw decoded value each
+// point is clamped against is the item's own F value before its write when
+// the field is the decoded field itself, else gathered per list entry when
+// the lists are built.  Floating-point expressions use explicit round-to-nearest
 // intrinsics so that no multiply-add is contracted (the reference host code is
 // compiled without contraction).
 #include <cfloat>
