@@ -66,7 +66,6 @@ __device__ __forceinline__ unsigned cta_excl_scan_post(unsigned v, unsigned *s_w
 constexpr int kPostThreads = 256;
 constexpr int kPostPer = 8;
 constexpr int kPostTile = kPostThreads * kPostPer;
-constexpr unsigned char kCandFlag = 0x80;
 
 __constant__ double c_w2[9];
 __constant__ double c_w3[27];
@@ -122,11 +121,6 @@ __device__ __forceinline__ C3 coords(const Geom &g, long long e) {
   else { c.x = fdivmod(e, g.plane, g.m_plane, r); c.y = fdivmod(r, g.d3, g.m_d3, c.z); }
   return c;
 }
-__device__ __forceinline__ bool interior(const Geom &g, const C3 &c) {
-  if (c.y < 1 || c.y > g.d2 - 2 || c.z < 1 || c.z > g.d3 - 2) return false;
-  if (g.nd == 3 && (c.x < 1 || c.x > g.d1 - 2)) return false;
-  return true;
-}
 
 // 4/6-neighbour classification on F (stable during a pass)
 __device__ __forceinline__ int classify_F(const PostArgs &a, long long q) {
@@ -153,11 +147,6 @@ __device__ __forceinline__ bool interior_off(const PostArgs &a, const C3 &c, int
   bool qi = c.y + dy >= 1 && c.y + dy <= a.g.d2 - 2 && c.z + dz >= 1 && c.z + dz <= a.g.d3 - 2;
   if (a.g.nd == 3) qi = qi && c.x + dx >= 1 && c.x + dx <= a.g.d1 - 2;
   return qi;
-}
-
-// candidate q has its result for the current pass
-__device__ __forceinline__ bool result_ready(const PostArgs &a, long long q) {
-  return (unsigned)(ld_rlx(&a.S[q]) >> 32) == a.gen;
 }
 
 // neighbour of e at offset (dx, dy, dz) (dx = 0 in 2D) as the serial pass
