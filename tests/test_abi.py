@@ -42,3 +42,11 @@ def test_version_string_without_gpu(libpath):
     lib = ctypes.CDLL(libpath)
     lib.szp_b200_version.restype = ctypes.c_char_p
     assert b"sm_100a" in lib.szp_b200_version()
+
+
+def test_batch_reserve_checks_its_arguments_without_gpu(libpath):
+    """szp_b200_batch_reserve validates on the host before any device call."""
+    import toposzp_b200 as T
+    L = T.lib()
+    assert L.szp_b200_batch_reserve(None, 4, 1 << 20) == -1
+    assert "invalid arguments" in T.last_error()
