@@ -521,8 +521,9 @@ SZP_B200_API double szp_b200_server_now(szp_b200_server *s);
  * elements, and its batch compressor for the largest merged launch (up to
  * max_batch fields of 2^24 elements in total), so that serving them allocates
  * nothing (an allocation while other workers run would stall the device for
- * all of them).  Call it while no request is in flight.  Returns 0 on
- * success. */
+ * all of them).  A relative-bound compression of more than 2^24 elements runs
+ * as a batch of one and still grows its worker's batch compressor the first
+ * time.  Call it while no request is in flight.  Returns 0 on success. */
 SZP_B200_API int szp_b200_server_reserve(szp_b200_server *s, size_t max_elements);
 SZP_B200_API int szp_b200_server_submit(szp_b200_server *s, szp_b200_request *r);
 /* 0 when r finished within timeout_s, 1 on timeout */
